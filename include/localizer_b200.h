@@ -1,0 +1,226 @@
+/*
+ * localizer_b200 — C ABI of the B200 Gaussian localization engine.
+ *
+ * Drop-in for the per-emitter Levenberg-Marquardt fitting path of Localizer:
+ * the FitPositions_* family (reference source/Localization.h:55-121,
+ * source/Localization.cpp:43-631), with the same method codes, PSF-width and
+ * noise-weight inputs, ROI half-width rule and output position columns
+ * (source/Storage.cpp:268-290, 405-425, 614-640). Plain pointers and sizes
+ * only; device pointers are CUDA global-memory addresses on the context's
+ * device, streams are cudaStream_t passed as void*.
+ *
+ * Error convention (mirrors LocalizerDLL, source/LocalizerDLL.cpp:124-128,
+ * where every failure returns -1): every int-returning call returns 0 on
+ * success and a negative LOC_E* code on failure; loc_last_error() gives a
+ * thread-local message for the last failure on the calling thread.
+ */
+#ifndef LOCALIZER_B200_H
+#define LOCALIZER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define LOC_API __declspec(dllexport)
+#else
+#define LOC_API __attribute__((visibility("default")))
+#endif
+
+/* Method codes: LOCALIZATION_METHOD_* of source/Defines.h:157-163. */
+#define LOC_METHOD_2DGAUSS 0                          /* FitPositions_SymmetricGaussian */
+#define LOC_METHOD_2DGAUSS_FIXEDWIDTH 1               /* FitPositions_FixedWidthGaussian */
+#define LOC_METHOD_2DGAUSS_ELLIPSOIDAL 5              /* FitPositions_EllipsoidalGaussian_SymmetricPSF */
+#define LOC_METHOD_2DGAUSS_ELLIPSOIDAL_ASTIGMATISM 7  /* FitPositions_EllipsoidalGaussian */
+
+/* Per-candidate reject codes (0 = kept: the candidate produced an output row
+ * in the reference). Each names the reference check that erases it. */
+#define LOC_FLAG_KEPT 0
+#define LOC_FLAG_EDGE 1            /* ROI leaves the frame, Localization.cpp:120 */
+#define LOC_FLAG_AMPLITUDE 2       /* fitted amplitude <= 0, :160 */
+#define LOC_FLAG_OUT_OF_WINDOW 3   /* fitted centre outside the ROI, :166 */
+#define LOC_FLAG_WIDTH_RANGE 4     /* symmetric width outside [0.4, 1.5] w0, :179 */
+#define LOC_FLAG_DRIFT 5           /* fixed width: centre moved > 2 w0, :349 */
+#define LOC_FLAG_EIGEN 6           /* ellipsoid eigen-decomposition failed, :534 */
+#define LOC_FLAG_NO_AXIS 7         /* no ellipsoid axis in [0.4, 1.5] w0, :550 */
+#define LOC_FLAG_SYMPSF_RATIO 8    /* method 5: axis ratio outside [0.75, 1.25], :616 */
+#define LOC_FLAG_SYMPSF_WIDTH 9    /* method 5: no axis in [0.7, 1.3] w0, :621 */
+#define LOC_FLAG_BAD_INPUT 10      /* frame index out of range or non-finite candidate */
+
+/* Termination status column (the value of the reference's solver loop at
+ * exit, Localization.cpp:148-155): 0 converged (test_delta), 1 iteration
+ * cap reached, otherwise the solver's stop code (GSL errno numbering:
+ * 9 bad function value, 27 no progress, 29/30/31 tolerance too small). */
+#define LOC_TERM_CONVERGED 0
+#define LOC_TERM_MAX_ITER 1
+
+/* Error codes. */
+#define LOC_OK 0
+#define LOC_E_INVALID -1      /* bad argument */
+#define LOC_E_CUDA -2         /* CUDA runtime error */
+#define LOC_E_NOMEM -3        /* device or host allocation failed */
+#define LOC_E_UNSUPPORTED -4  /* method / size outside what this build handles */
+#define LOC_E_DEVICE -5       /* a kernel reported an error word */
+
+#define LOC_MAX_HALF_WIDTH 16 /* largest ROI half-width r (ROI (2r+1)^2) */
+
+/* Candidate emitter: the reference's Particle (source/Storage.h:90-101,
+ * produced by the particle finders, source/ParticleFinding.cpp:351-377)
+ * plus the frame it belongs to and an optional ROI half-width override.
+ * half_width == 0 selects the reference rule r = ceil(4 * w0)
+ * (source/Localization.h:68). 40 bytes, 8-byte aligned. */
+typedef struct loc_candidate {
+    double x;            /* pixel coordinate along rows (fastest image axis) */
+    double y;            /* pixel coordinate along columns */
+    double intensity;    /* initial amplitude */
+    double background;   /* initial offset */
+    int32_t frame;       /* index into the frame stack */
+    int32_t half_width;  /* ROI half-width r, or 0 for ceil(4*w0) */
+} loc_candidate;
+
+/* Precision of the iterative solve. FP32 is the production path (FP32
+ * model, Jacobian and normal equations; FP64 only for ill-conditioned
+ * Cholesky pivots and for the final covariance). FP64 runs the same
+ * algorithm entirely in double precision (for accuracy studies). */
+#define LOC_PRECISION_FP32 0
+#define LOC_PRECISION_FP64 1
+
+typedef struct loc_options {
+    int32_t max_iter;          /* solver iteration cap; 200 in the reference */
+    double epsabs;             /* test_delta absolute tolerance; 1e-4 */
+    double epsrel;             /* test_delta relative tolerance; 1e-4 */
+    int32_t precision;         /* LOC_PRECISION_* */
+    float pivot_threshold;     /* FP32 Cholesky pivots below this fraction of
+                                  their diagonal are redone in FP64; 1e-4 */
+    int32_t threads_per_block; /* 0: tuned default */
+    int32_t blocks_per_sm;     /* 0: occupancy maximum */
+    int32_t stage_u16;         /* -1: tuned; 0: ROI staged as float; 1: as uint16 */
+    int32_t max_half_width;    /* 0: the solver reads the largest ROI half-width
+                                  present back from the device (one small
+                                  synchronous copy); > 0: caller guarantees
+                                  every candidate's r is at most this (no host
+                                  synchronisation, capturable in a CUDA graph);
+                                  larger candidates are flagged LOC_FLAG_BAD_INPUT */
+    const float *d_init_params;/* optional device array, n_cands x p floats of
+                                  absolute-coordinate start parameters (warm
+                                  start); NULL = reference start values */
+    float *d_params_out;       /* optional device array, n_cands x p floats:
+                                  raw fitted parameters (absolute coordinates) */
+} loc_options;
+
+/* Fills *opt with the reference's defaults. */
+LOC_API void loc_default_options(loc_options *opt);
+
+typedef struct loc_ctx loc_ctx;
+
+/* Create a context on CUDA device `device` (device memory pools, tuned
+ * launch shapes, counters). The context is not thread-safe; use one per
+ * host thread. */
+LOC_API int loc_ctx_create(loc_ctx **ctx, int device);
+LOC_API int loc_ctx_destroy(loc_ctx *ctx);
+
+/* Thread-local description of the last failure on this thread. */
+LOC_API const char *loc_last_error(void);
+
+/* Number of reference output columns for a method (12 / 10 / 16), or a
+ * negative error. Rows written by the fit calls carry two more columns:
+ * the solver's iteration count and the termination status. */
+LOC_API int loc_reference_columns(int method);
+LOC_API int loc_output_columns(int method);
+
+/* Number of fitted parameters for a method (5 / 4 / 7). */
+LOC_API int loc_parameter_count(int method);
+
+/*
+ * Fit every candidate of a frame stack on the GPU (the batched
+ * FitPositions::fit_positions, reference source/Localization.h:60, called
+ * per frame at source/PALMAnalysis.cpp:234).
+ *
+ * d_frames: n_frames x n_cols x n_rows uint16, x fastest (frame f, pixel
+ *           (x, y) at f*n_rows*n_cols + x + y*n_rows), as the reference
+ *           lays out images (source/Defines.h:44, source/FileIO.cpp:195).
+ * d_cands:  n_cands candidates (any order; any frames).
+ * d_out:    n_cands rows of loc_output_columns(method) doubles, one row per
+ *           candidate in submission order. Rows of kept candidates hold the
+ *           reference's columns; the reference columns of rejected rows are
+ *           NaN except column 0 (frame).
+ * d_flags:  n_cands reject codes (LOC_FLAG_*).
+ * w0:       initialPSFWidth (> 0); sigma: the noise weight (non-zero).
+ * Asynchronous on `stream`; device errors are reported by the next call or
+ * by loc_sync.
+ */
+LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, int n_rows,
+                          int n_cols, const loc_candidate *d_cands, int n_cands, int method,
+                          double w0, double sigma, const loc_options *opt, double *d_out,
+                          uint8_t *d_flags, void *stream);
+
+/* Same fit with host buffers: copies frames and candidates to the device,
+ * fits and copies rows and flags back (the whole path a host caller sees). */
+LOC_API int loc_fit_host(loc_ctx *ctx, const uint16_t *frames, int n_frames, int n_rows,
+                         int n_cols, const loc_candidate *cands, int n_cands, int method,
+                         double w0, double sigma, const loc_options *opt, double *out,
+                         uint8_t *flags);
+
+/* Wait for all work of the context on `stream` and report device errors. */
+LOC_API int loc_sync(loc_ctx *ctx, void *stream);
+
+/* Counters of the last fit call (after loc_sync): trial-point evaluations,
+ * Jacobian evaluations, damped Cholesky solves, FP64 pivot escalations,
+ * candidates enqueued and total solver iterations. */
+typedef struct loc_stats {
+    uint64_t f_evals;
+    uint64_t jacobian_evals;
+    uint64_t lambda_solves;
+    uint64_t fp64_escalations;
+    uint64_t fits;
+    uint64_t iterations;
+    uint64_t pixels_f;     /* sum over trial evaluations of ROI pixels */
+    uint64_t pixels_j;     /* sum over Jacobian evaluations of ROI pixels */
+} loc_stats;
+LOC_API int loc_last_stats(loc_ctx *ctx, loc_stats *stats);
+
+/*
+ * Reference output matrix of the kept rows: the N x C double matrix that
+ * getLocalizedPositionsAsMatrix() returns (Storage.cpp:268-290, 405-425,
+ * 614-640), rows in submission order (the reference sorts by frame,
+ * PALMAnalysis.cpp:188, so submit candidates in frame order), stored
+ * column-major like the reference's Eigen matrix. Host buffers.
+ * Returns the number of kept rows, or a negative error; writes at most
+ * max_rows rows.
+ */
+LOC_API int loc_compact_host(const double *out, const uint8_t *flags, int n_cands, int method,
+                             double *matrix, int max_rows);
+
+/*
+ * Candidate finder on one frame stack (host): the GLRT detector
+ * (ThresholdImage_GLRT_FFT, source/Segmentation.cpp:241-430) followed by the
+ * adjacent-8 particle finder (source/ParticleFinding.cpp:283-427), one
+ * loc_candidate per particle in frame order, half_width 0.
+ * Returns the number of candidates found (may exceed max_cands; only
+ * max_cands are written) or a negative error.
+ */
+LOC_API long loc_find_candidates_host(const uint16_t *frames, int n_frames, int n_rows,
+                                      int n_cols, double pfa, double psf_width, int n_threads,
+                                      loc_candidate *cands, long max_cands);
+
+/*
+ * Compatibility entry points with the signatures of the reference DLL
+ * (source/LocalizerDLL.h:53-56): GLRT + adjacent-8 candidates, then the
+ * ellipsoidal fit (FitPositions_EllipsoidalGaussian(psfWidth, 1.0),
+ * LocalizerDLL.cpp:107) on the GPU; *emitterCoordinates receives the
+ * N x 16 column-major matrix, allocated by the callee; release it with
+ * LocalizerFree. Returns 0 or -1, as the reference does.
+ */
+LOC_API int LocalizerFitEmitters(unsigned short *imageData, int nRows, int nCols, int nImages,
+                                 double psfWidth, double glrtInsensitivity, int *nEmitters,
+                                 double **emitterCoordinates);
+LOC_API void LocalizerFree(double *ptrToFree);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,337 @@
+// C ABI of the B200 localization engine (declared in include/localizer_b200.h).
+#include "../../include/localizer_b200.h"
+#include "loc_fit.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *where)
+{
+    return fail(LOC_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+int method_ok(int m) { return m == 0 || m == 1 || m == 5 || m == 7; }
+
+// Device buffer that grows on demand.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes)
+    {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = bytes + bytes / 8 + 4096;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+}  // namespace
+
+struct loc_ctx {
+    int device = 0;
+    DevBuf scratch;
+    // device copies for the host-buffer path
+    DevBuf frames, cands, out, flags;
+    unsigned long long *stats_dev = nullptr;  // points into scratch of the last call
+    loc_stats last{};
+    bool stats_valid = false;
+};
+
+extern "C" {
+
+LOC_API const char *loc_last_error(void) { return g_err.c_str(); }
+
+LOC_API void loc_default_options(loc_options *opt)
+{
+    if (!opt) return;
+    std::memset(opt, 0, sizeof(*opt));
+    opt->max_iter = 200;   // Localization.cpp:155
+    opt->epsabs = 1e-4;    // Localization.cpp:154
+    opt->epsrel = 1e-4;
+    opt->precision = LOC_PRECISION_FP32;
+    opt->pivot_threshold = 1e-4f;
+    opt->threads_per_block = 0;
+    opt->blocks_per_sm = 0;
+    opt->stage_u16 = -1;
+    opt->max_half_width = 0;
+}
+
+LOC_API int loc_reference_columns(int method)
+{
+    if (!method_ok(method)) return fail(LOC_E_UNSUPPORTED, "unsupported method code");
+    return method == 0 ? 12 : method == 1 ? 10 : 16;
+}
+
+LOC_API int loc_output_columns(int method)
+{
+    int c = loc_reference_columns(method);
+    return c < 0 ? c : c + 2;
+}
+
+LOC_API int loc_parameter_count(int method)
+{
+    if (!method_ok(method)) return fail(LOC_E_UNSUPPORTED, "unsupported method code");
+    return method == 0 ? 5 : method == 1 ? 4 : 7;
+}
+
+LOC_API int loc_ctx_create(loc_ctx **ctx, int device)
+{
+    if (!ctx) return fail(LOC_E_INVALID, "ctx is NULL");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
+    if (device < 0 || device >= n) return fail(LOC_E_INVALID, "device index out of range");
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    loc_ctx *c = new (std::nothrow) loc_ctx();
+    if (!c) return fail(LOC_E_NOMEM, "context allocation failed");
+    c->device = device;
+    *ctx = c;
+    return LOC_OK;
+}
+
+LOC_API int loc_ctx_destroy(loc_ctx *ctx)
+{
+    if (!ctx) return LOC_OK;
+    cudaSetDevice(ctx->device);
+    ctx->scratch.release();
+    ctx->frames.release();
+    ctx->cands.release();
+    ctx->out.release();
+    ctx->flags.release();
+    delete ctx;
+    return LOC_OK;
+}
+
+static int validate(const loc_ctx *ctx, const void *frames, int n_frames, int n_rows, int n_cols,
+                    const void *cands, int n_cands, int method, double w0, double sigma, const void *out,
+                    const void *flags)
+{
+    if (!ctx) return fail(LOC_E_INVALID, "ctx is NULL");
+    if (!method_ok(method)) return fail(LOC_E_UNSUPPORTED, "unsupported method code");
+    if (n_cands < 0) return fail(LOC_E_INVALID, "n_cands < 0");
+    if (n_cands > 0 && (!cands || !out || !flags)) return fail(LOC_E_INVALID, "NULL buffer");
+    if (n_frames < 0 || n_rows <= 0 || n_cols <= 0) return fail(LOC_E_INVALID, "bad frame stack shape");
+    if (n_frames > 0 && !frames) return fail(LOC_E_INVALID, "frames is NULL");
+    if (!(w0 > 0) || !std::isfinite(w0)) return fail(LOC_E_INVALID, "w0 must be finite and > 0");
+    if (!(sigma != 0) || !std::isfinite(sigma)) return fail(LOC_E_INVALID, "sigma must be finite and non-zero");
+    return LOC_OK;
+}
+
+LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, int n_rows, int n_cols,
+                          const loc_candidate *d_cands, int n_cands, int method, double w0, double sigma,
+                          const loc_options *opt, double *d_out, uint8_t *d_flags, void *stream)
+{
+    int rc = validate(ctx, d_frames, n_frames, n_rows, n_cols, d_cands, n_cands, method, w0, sigma, d_out, d_flags);
+    if (rc) return rc;
+    loc_options o;
+    if (opt) o = *opt;
+    else loc_default_options(&o);
+    if (o.max_iter < 1) return fail(LOC_E_INVALID, "max_iter < 1");
+    if (!(o.epsrel >= 0) || !(o.epsabs >= 0)) return fail(LOC_E_INVALID, "negative tolerance");
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    const size_t need = locb::scratch_bytes(method, n_cands);
+    e = ctx->scratch.ensure(need);
+    if (e != cudaSuccess) return fail(LOC_E_NOMEM, std::string("scratch allocation: ") + cudaGetErrorString(e));
+    locb::Scratch s;
+    locb::carve_scratch(ctx->scratch.p, method, n_cands, &s);
+    locb::FitParams p{};
+    p.frames = d_frames;
+    p.n_frames = n_frames;
+    p.n_rows = n_rows;
+    p.n_cols = n_cols;
+    p.cands = d_cands;
+    p.n_cands = n_cands;
+    p.method = method;
+    p.w0 = w0;
+    p.sigma = sigma;
+    p.max_iter = o.max_iter;
+    p.epsabs = o.epsabs;
+    p.epsrel = o.epsrel;
+    p.precision = o.precision;
+    p.pivot_thr = o.pivot_threshold > 0 ? o.pivot_threshold : 1e-4f;
+    p.threads_per_block = o.threads_per_block;
+    p.blocks_per_sm = o.blocks_per_sm;
+    p.max_half_width = o.max_half_width;
+    p.init_params = o.d_init_params;
+    p.params_out = o.d_params_out;
+    p.out = d_out;
+    p.flags = d_flags;
+    int detail = 0;
+    e = locb::enqueue_fit(p, s, (cudaStream_t)stream, &detail);
+    ctx->stats_dev = s.stats;
+    ctx->stats_valid = false;
+    if (e != cudaSuccess) {
+        if (detail == 1) return fail(LOC_E_UNSUPPORTED, "ROI too large for shared memory");
+        return cuda_fail(e, "fit launch");
+    }
+    return LOC_OK;
+}
+
+LOC_API int loc_sync(loc_ctx *ctx, void *stream)
+{
+    if (!ctx) return fail(LOC_E_INVALID, "ctx is NULL");
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "stream synchronize");
+    return LOC_OK;
+}
+
+LOC_API int loc_last_stats(loc_ctx *ctx, loc_stats *st)
+{
+    if (!ctx || !st) return fail(LOC_E_INVALID, "NULL argument");
+    if (!ctx->stats_dev) {
+        std::memset(st, 0, sizeof(*st));
+        return LOC_OK;
+    }
+    unsigned long long v[8];
+    cudaError_t e = cudaMemcpy(v, ctx->stats_dev, sizeof(v), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "stats copy");
+    st->f_evals = v[0];
+    st->jacobian_evals = v[1];
+    st->lambda_solves = v[2];
+    st->fp64_escalations = v[3];
+    st->fits = v[4];
+    st->iterations = v[5];
+    st->pixels_f = v[6];
+    st->pixels_j = v[7];
+    return LOC_OK;
+}
+
+LOC_API int loc_fit_host(loc_ctx *ctx, const uint16_t *frames, int n_frames, int n_rows, int n_cols,
+                         const loc_candidate *cands, int n_cands, int method, double w0, double sigma,
+                         const loc_options *opt, double *out, uint8_t *flags)
+{
+    int rc = validate(ctx, frames, n_frames, n_rows, n_cols, cands, n_cands, method, w0, sigma, out, flags);
+    if (rc) return rc;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    const size_t fbytes = (size_t)n_frames * n_rows * n_cols * sizeof(uint16_t);
+    const size_t cbytes = (size_t)n_cands * sizeof(loc_candidate);
+    const int ncol = loc_output_columns(method);
+    const size_t obytes = (size_t)n_cands * ncol * sizeof(double);
+    if ((e = ctx->frames.ensure(fbytes ? fbytes : 1)) != cudaSuccess ||
+        (e = ctx->cands.ensure(cbytes ? cbytes : 1)) != cudaSuccess ||
+        (e = ctx->out.ensure(obytes ? obytes : 1)) != cudaSuccess ||
+        (e = ctx->flags.ensure(n_cands ? n_cands : 1)) != cudaSuccess)
+        return fail(LOC_E_NOMEM, std::string("device buffers: ") + cudaGetErrorString(e));
+    cudaStream_t st = 0;
+    if (fbytes && (e = cudaMemcpyAsync(ctx->frames.p, frames, fbytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return cuda_fail(e, "frames upload");
+    if (cbytes && (e = cudaMemcpyAsync(ctx->cands.p, cands, cbytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return cuda_fail(e, "candidates upload");
+    rc = loc_fit_batch(ctx, (const uint16_t *)ctx->frames.p, n_frames, n_rows, n_cols,
+                       (const loc_candidate *)ctx->cands.p, n_cands, method, w0, sigma, opt, (double *)ctx->out.p,
+                       (uint8_t *)ctx->flags.p, st);
+    if (rc) return rc;
+    if (obytes && (e = cudaMemcpyAsync(out, ctx->out.p, obytes, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(e, "rows download");
+    if (n_cands && (e = cudaMemcpyAsync(flags, ctx->flags.p, n_cands, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(e, "flags download");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "fit");
+    return LOC_OK;
+}
+
+LOC_API int loc_compact_host(const double *out, const uint8_t *flags, int n_cands, int method, double *matrix,
+                             int max_rows)
+{
+    const int rcols = loc_reference_columns(method);
+    if (rcols < 0) return rcols;
+    if (n_cands < 0 || (n_cands > 0 && (!out || !flags))) return fail(LOC_E_INVALID, "bad arguments");
+    const int ncol = rcols + 2;
+    int kept = 0;
+    for (int i = 0; i < n_cands; ++i) kept += flags[i] == LOC_FLAG_KEPT;
+    if (kept > max_rows || !matrix) return kept;
+    int row = 0;
+    for (int i = 0; i < n_cands; ++i) {
+        if (flags[i] != LOC_FLAG_KEPT) continue;
+        for (int c = 0; c < rcols; ++c) matrix[(size_t)c * kept + row] = out[(size_t)i * ncol + c];
+        ++row;
+    }
+    return kept;
+}
+
+}  // extern "C"
+
+// ---- reference DLL compatibility (LocalizerDLL.h:53-56) ----
+
+namespace {
+std::mutex g_compat_mu;
+loc_ctx *g_compat_ctx = nullptr;
+}  // namespace
+
+extern "C" {
+
+LOC_API int LocalizerFitEmitters(unsigned short *imageData, int nRows, int nCols, int nImages, double psfWidth,
+                                 double glrtInsensitivity, int *nEmitters, double **emitterCoordinates)
+{
+    try {
+        if (!imageData || !nEmitters || !emitterCoordinates || nRows <= 0 || nCols <= 0 || nImages < 0) return -1;
+        std::lock_guard<std::mutex> lk(g_compat_mu);
+        if (!g_compat_ctx) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            if (loc_ctx_create(&g_compat_ctx, dev) != LOC_OK) return -1;
+        }
+        // candidates: GLRT (PFA = glrtInsensitivity, width = psfWidth) + adjacent-8, as LocalizerDLL.cpp:99-103
+        long cap = 1 << 16;
+        std::vector<loc_candidate> cands;
+        long n = 0;
+        for (;;) {
+            cands.resize((size_t)cap);
+            n = loc_find_candidates_host(imageData, nImages, nRows, nCols, glrtInsensitivity, psfWidth, 0,
+                                         cands.data(), cap);
+            if (n < 0) return -1;
+            if (n <= cap) break;
+            cap = n;
+        }
+        cands.resize((size_t)n);
+        const int method = LOC_METHOD_2DGAUSS_ELLIPSOIDAL_ASTIGMATISM;  // LocalizerDLL.cpp:107
+        const int ncol = loc_output_columns(method);
+        std::vector<double> out((size_t)n * ncol);
+        std::vector<uint8_t> flags((size_t)n);
+        if (n > 0 && loc_fit_host(g_compat_ctx, imageData, nImages, nRows, nCols, cands.data(), (int)n, method,
+                                  psfWidth, 1.0, nullptr, out.data(), flags.data()) != LOC_OK)
+            return -1;
+        int kept = loc_compact_host(out.data(), flags.data(), (int)n, method, nullptr, 0);
+        if (kept < 0) return -1;
+        double *m = new double[(size_t)kept * 16 + 1];
+        loc_compact_host(out.data(), flags.data(), (int)n, method, m, kept);
+        *nEmitters = kept;
+        *emitterCoordinates = m;
+    } catch (...) {
+        return -1;
+    }
+    return 0;
+}
+
+LOC_API void LocalizerFree(double *ptrToFree) { delete[] ptrToFree; }
+
+}  // extern "C"

@@ -1,0 +1,423 @@
+// Device building blocks of the B200 Levenberg-Marquardt fit engine.
+//
+// One CUDA thread owns one emitter fit ("lane"); a warp advances 32 fits in
+// lock step, one model evaluation pass per loop trip. The iteration is the
+// scaled trust-region Levenberg-Marquardt method that the reference runs
+// through GSL's lmsder (source/Localization.cpp:145-155; GSL 1.16, MINPACK
+// lmder/lmpar of More 1978), restated on the normal equations: every pass
+// accumulates J^T J, J^T f and |f|^2 of the ROI, and the damped step
+// (J^T J + par D^2) p = -J^T f of MINPACK's lmpar is solved by an in-register
+// Cholesky factorisation of the D-scaled matrix. In exact arithmetic this
+// is the same sequence of steps, trust radii and Levenberg parameters as the
+// QR-based lmsder; FP32 pivots that fall below a conditioning threshold are
+// refactorised in FP64.
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace locb {
+
+struct Cand {
+    double x, y, intensity, background;
+    int32_t frame;
+    int32_t half_width;
+};
+static_assert(sizeof(Cand) == 40, "candidate layout");
+
+// Parameter vectors per method (reference Localization.cpp:138-142, 318-321,
+// 485-491): symmetric (A, s, x0, y0, b); fixed width (A, x0, y0, b);
+// ellipsoidal (A, sx, sy, x0, y0, rho, b). IX = index of x0.
+template <int METHOD> struct Traits;
+template <> struct Traits<0> { static constexpr int P = 5; static constexpr int IX = 2; };
+template <> struct Traits<1> { static constexpr int P = 4; static constexpr int IX = 1; };
+template <> struct Traits<7> { static constexpr int P = 7; static constexpr int IX = 3; };
+
+__host__ __device__ constexpr int tri(int P) { return P * (P + 1) / 2; }
+// packed upper triangle (row-major, i <= j)
+__host__ __device__ constexpr int pku(int P, int i, int j) { return i * P - i * (i - 1) / 2 + (j - i); }
+// packed lower triangle (row-major, j <= i)
+__host__ __device__ constexpr int pkl(int i, int j) { return i * (i + 1) / 2 + j; }
+
+// Per-candidate fit state handed from the solver kernel to the finaliser.
+// Floats: [0,P) parameters (ROI-local positions), [P, P+NT) scaled J^T J,
+// then fnorm, iterations, status, x_off, y_off (ints stored bitwise).
+template <int P> struct StateLayout {
+    static constexpr int NT = tri(P);
+    static constexpr int FNORM = P + NT;
+    static constexpr int ITERS = FNORM + 1;
+    static constexpr int STATUS = FNORM + 2;
+    static constexpr int XOFF = FNORM + 3;
+    static constexpr int YOFF = FNORM + 4;
+    static constexpr int STRIDE = ((FNORM + 5) + 3) / 4 * 4;
+};
+
+// Reject codes and termination codes (public header LOC_FLAG_*, LOC_TERM_*).
+enum : uint8_t {
+    F_KEPT = 0, F_EDGE = 1, F_AMPLITUDE = 2, F_WINDOW = 3, F_WIDTH = 4, F_DRIFT = 5,
+    F_EIGEN = 6, F_NO_AXIS = 7, F_SYM_RATIO = 8, F_SYM_WIDTH = 9, F_BAD_INPUT = 10,
+    F_PENDING = 255
+};
+enum : int { T_CONVERGED = 0, T_MAX_ITER = 1, T_EBADFUNC = 9, T_ENOPROG = 27, T_ETOLF = 29,
+             T_ETOLX = 30, T_ETOLG = 31, T_SINGULAR = 64 };
+
+// stats slots
+enum { ST_F = 0, ST_J = 1, ST_LAMBDA = 2, ST_ESC = 3, ST_FITS = 4, ST_ITERS = 5, ST_PIXF = 6,
+       ST_PIXJ = 7, ST_N = 8 };
+
+constexpr double kDblEps = 2.2204460492503131e-16;   // GSL_DBL_EPSILON
+constexpr float kLog2e = 1.4426950408889634f;
+
+__device__ __forceinline__ float ex2_approx(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// exp(-c*q) in the precision of T. For float the constant is pre-multiplied
+// by log2(e) and the hardware exp2 unit is used; for double, exp().
+template <typename T> struct Expo;
+template <> struct Expo<float> {
+    static constexpr float scale = kLog2e;
+    __device__ __forceinline__ static float ex(float a) { return ex2_approx(a); }
+};
+template <> struct Expo<double> {
+    static constexpr double scale = 1.0;
+    __device__ __forceinline__ static double ex(double a) { return exp(a); }
+};
+
+template <typename T> __device__ __forceinline__ T tiny_pos();
+template <> __device__ __forceinline__ float tiny_pos<float>() { return FLT_MIN; }
+template <> __device__ __forceinline__ double tiny_pos<double>() { return DBL_MIN; }
+
+// ---------------------------------------------------------------------------
+// Model + Jacobian + normal-equation accumulation over one ROI.
+//
+// roi: this lane's pixels in shared memory, pixel k = i + j*S at roi[k*ld]
+// (i along x). Parameters are ROI-local (x0 measured from the ROI origin).
+// acc receives the packed upper triangle of J^T J without its last entry
+// (the offset column is identically 1, so that entry is the pixel count),
+// vv = J^T r and chi2 = |r|^2, with r = model - data (unit noise weight;
+// the caller rescales). Expressions follow the reference callbacks:
+// symmetric Localization.cpp:1007-1048 / 1128-1181 (width column scaled by
+// 1/sqrt(2) as in the reference), fixed width :1050-1076 / 1183-1225,
+// ellipsoidal :1078-1126 / 1227-1295 (correlation column as written there).
+// ---------------------------------------------------------------------------
+
+template <typename T, typename R>
+__device__ __forceinline__ T load_px(const R *roi, int k, int ld);
+template <>
+__device__ __forceinline__ float load_px<float, float>(const float *roi, int k, int ld) { return roi[k * ld]; }
+template <>
+__device__ __forceinline__ double load_px<double, float>(const float *roi, int k, int ld) { return (double)roi[k * ld]; }
+
+// S > 0: compile-time ROI side (rows fully unrolled); S == 0: runtime side s_rt.
+template <int S, typename T>
+__device__ __forceinline__ void pass_sym(const float *__restrict__ roi, int ld, int s_rt,
+                                         const T (&th)[5], T (&acc)[14], T (&vv)[5], T &chi2)
+{
+    const int s = S > 0 ? S : s_rt;
+    const T A = th[0], w = th[1], x0 = th[2], y0 = th[3], b = th[4];
+    const T w2i = T(1) / (w * w);
+    const T c1 = -T(0.5) * w2i * (T)Expo<T>::scale;
+    const T ka_x = A * w2i;                                   // dfdx0 = u e A / w^2
+    const T ka_r = ka_x / (w * T(1.4142135623730950488));      // dfdr = d2 e A / (sqrt2 w^3)
+#pragma unroll
+    for (int k = 0; k < 14; ++k) acc[k] = T(0);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) vv[k] = T(0);
+    chi2 = T(0);
+    auto body = [&](int i, T wy, T wy2, const float *row) {
+        const T u = (T)i - x0;
+        const T d2 = fma(u, u, wy2);
+        const T e = Expo<T>::ex(d2 * c1);
+        const T dat = load_px<T, float>(row, i, ld);
+        const T r = fma(A, e, b - dat);
+        const T jr = d2 * (e * ka_r);
+        const T ex = e * ka_x;
+        const T jx = u * ex, jy = wy * ex;
+        acc[0] = fma(e, e, acc[0]);   acc[1] = fma(e, jr, acc[1]);   acc[2] = fma(e, jx, acc[2]);
+        acc[3] = fma(e, jy, acc[3]);  acc[4] += e;
+        acc[5] = fma(jr, jr, acc[5]); acc[6] = fma(jr, jx, acc[6]); acc[7] = fma(jr, jy, acc[7]);
+        acc[8] += jr;
+        acc[9] = fma(jx, jx, acc[9]); acc[10] = fma(jx, jy, acc[10]); acc[11] += jx;
+        acc[12] = fma(jy, jy, acc[12]); acc[13] += jy;
+        vv[0] = fma(e, r, vv[0]); vv[1] = fma(jr, r, vv[1]); vv[2] = fma(jx, r, vv[2]);
+        vv[3] = fma(jy, r, vv[3]); vv[4] += r;
+        chi2 = fma(r, r, chi2);
+    };
+#pragma unroll 1
+    for (int j = 0; j < s; ++j) {
+        const T wy = (T)j - y0;
+        const T wy2 = wy * wy;
+        const float *row = roi + j * s * ld;
+        if (S > 0) {
+#pragma unroll
+            for (int i = 0; i < (S > 0 ? S : 1); ++i) body(i, wy, wy2, row);
+        } else {
+#pragma unroll 1
+            for (int i = 0; i < s; ++i) body(i, wy, wy2, row);
+        }
+    }
+}
+
+template <int S, typename T>
+__device__ __forceinline__ void pass_fixed(const float *__restrict__ roi, int ld, int s_rt, T w0,
+                                           const T (&th)[4], T (&acc)[9], T (&vv)[4], T &chi2)
+{
+    const int s = S > 0 ? S : s_rt;
+    const T A = th[0], x0 = th[1], y0 = th[2], b = th[3];
+    const T w2i = T(1) / (w0 * w0);
+    const T c1 = -T(0.5) * w2i * (T)Expo<T>::scale;
+    const T ka_x = A * w2i;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) acc[k] = T(0);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) vv[k] = T(0);
+    chi2 = T(0);
+    auto body = [&](int i, T wy, T wy2, const float *row) {
+        const T u = (T)i - x0;
+        const T d2 = fma(u, u, wy2);
+        const T e = Expo<T>::ex(d2 * c1);
+        const T dat = load_px<T, float>(row, i, ld);
+        const T r = fma(A, e, b - dat);
+        const T ex = e * ka_x;
+        const T jx = u * ex, jy = wy * ex;
+        acc[0] = fma(e, e, acc[0]); acc[1] = fma(e, jx, acc[1]); acc[2] = fma(e, jy, acc[2]); acc[3] += e;
+        acc[4] = fma(jx, jx, acc[4]); acc[5] = fma(jx, jy, acc[5]); acc[6] += jx;
+        acc[7] = fma(jy, jy, acc[7]); acc[8] += jy;
+        vv[0] = fma(e, r, vv[0]); vv[1] = fma(jx, r, vv[1]); vv[2] = fma(jy, r, vv[2]); vv[3] += r;
+        chi2 = fma(r, r, chi2);
+    };
+#pragma unroll 1
+    for (int j = 0; j < s; ++j) {
+        const T wy = (T)j - y0;
+        const T wy2 = wy * wy;
+        const float *row = roi + j * s * ld;
+        if (S > 0) {
+#pragma unroll
+            for (int i = 0; i < (S > 0 ? S : 1); ++i) body(i, wy, wy2, row);
+        } else {
+#pragma unroll 1
+            for (int i = 0; i < s; ++i) body(i, wy, wy2, row);
+        }
+    }
+}
+
+template <int S, typename T>
+__device__ __forceinline__ void pass_ell(const float *__restrict__ roi, int ld, int s_rt,
+                                         const T (&th)[7], T (&acc)[27], T (&vv)[7], T &chi2)
+{
+    const int s = S > 0 ? S : s_rt;
+    const T A = th[0], sx = th[1], sy = th[2], x0 = th[3], y0 = th[4], rho = th[5], b = th[6];
+    const T isx = T(1) / sx, isy = T(1) / sy;
+    const T a = isx * isx, c = isy * isy, bb = isx * isy;
+    const T rb = rho * bb;
+    const T k = T(1) / (T(1) - rho * rho);
+    const T cexp = -T(0.5) * k * (T)Expo<T>::scale;
+    const T AK = A * k;
+    const T ABK = AK * bb;
+    const T rk = rho * k;
+    const T tr = T(2) * rho;
+#pragma unroll
+    for (int q = 0; q < 27; ++q) acc[q] = T(0);
+#pragma unroll
+    for (int q = 0; q < 7; ++q) vv[q] = T(0);
+    chi2 = T(0);
+    auto body = [&](int i, T wy, T wy2, T wc, T wrb, const float *row) {
+        const T u = (T)i - x0;
+        const T P1 = fma(u, a, -wrb);            // u/sx^2 - rho w/(sx sy)
+        const T P2 = fma(-rb, u, wc);            // w/sy^2 - rho u/(sx sy)
+        const T q = fma(u, P1, wy * P2);         // the quadratic form
+        const T e = Expo<T>::ex(q * cexp);
+        const T dat = load_px<T, float>(row, i, ld);
+        const T r = fma(A, e, b - dat);
+        const T ek = e * AK;
+        const T jx = ek * P1, jy = ek * P2;      // dfdx0, dfdy0
+        const T jsx = (jx * u) * isx;            // dfdsigmaX
+        const T jsy = (jy * wy) * isy;           // dfdsigmaY
+        const T uw = u * wy;
+        const T d2 = fma(u, u, wy2);
+        const T inner = fma(-tr, uw, d2);
+        const T t = fma(-rk, inner, uw);
+        const T jrho = (e * ABK) * t;            // dfdcorr as in the reference
+        const T col[6] = {e, jsx, jsy, jx, jy, jrho};
+        int o = 0;
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+#pragma unroll
+            for (int n = m; n < 6; ++n) acc[o + n - m] = fma(col[m], col[n], acc[o + n - m]);
+            acc[o + 6 - m] += col[m];
+            o += 7 - m;
+        }
+#pragma unroll
+        for (int m = 0; m < 6; ++m) vv[m] = fma(col[m], r, vv[m]);
+        vv[6] += r;
+        chi2 = fma(r, r, chi2);
+    };
+#pragma unroll 1
+    for (int j = 0; j < s; ++j) {
+        const T wy = (T)j - y0;
+        const T wy2 = wy * wy;
+        const T wc = wy * c;
+        const T wrb = wy * rb;
+        const float *row = roi + j * s * ld;
+        if (S > 0) {
+#pragma unroll
+            for (int i = 0; i < (S > 0 ? S : 1); ++i) body(i, wy, wy2, wc, wrb, row);
+        } else {
+#pragma unroll 1
+            for (int i = 0; i < s; ++i) body(i, wy, wy2, wc, wrb, row);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Damped solve in D-scaled coordinates. With M = D^-1 J^T J D^-1 and
+// g = D^-1 J^T f, the lmpar step x (J x ~ f, reference step dx = -x) is
+// D x = z with (M + par I) z = g. Returns z, |z| and |L^-1 z|^2 / |z|^2
+// (the quantity MINPACK's lmpar forms as |w|^2 through R or S).
+// Result codes: 0 ok, 1 an FP32 pivot fell below thr * diagonal (redo in
+// FP64), 2 not positive definite (in the precision T).
+// ---------------------------------------------------------------------------
+template <int P, typename T, typename MS>
+__device__ __forceinline__ int chol_solve(const MS (&Ms)[tri(P)], MS par, const MS (&g)[P], T thr,
+                                          MS (&z)[P], MS &znorm, MS &w2)
+{
+    T L[tri(P)];
+    T inv[P];
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        const T djj = (T)Ms[pku(P, j, j)] + (T)par;
+        T d = djj;
+#pragma unroll
+        for (int k = 0; k < j; ++k) d -= L[pkl(j, k)] * L[pkl(j, k)];
+        if (!(d > thr * djj)) return thr > T(0) ? 1 : 2;
+        const T l = sqrt(d);
+        inv[j] = T(1) / l;
+        L[pkl(j, j)] = l;
+#pragma unroll
+        for (int i = j + 1; i < P; ++i) {
+            T sacc = (T)Ms[pku(P, j, i)];
+#pragma unroll
+            for (int k = 0; k < j; ++k) sacc -= L[pkl(i, k)] * L[pkl(j, k)];
+            L[pkl(i, j)] = sacc * inv[j];
+        }
+    }
+    T y[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+        T sacc = (T)g[i];
+#pragma unroll
+        for (int k = 0; k < i; ++k) sacc -= L[pkl(i, k)] * y[k];
+        y[i] = sacc * inv[i];
+    }
+    T zz[P];
+#pragma unroll
+    for (int ii = P - 1; ii >= 0; --ii) {
+        T sacc = y[ii];
+#pragma unroll
+        for (int k = ii + 1; k < P; ++k) sacc -= L[pkl(k, ii)] * zz[k];
+        zz[ii] = sacc * inv[ii];
+    }
+    T n2 = T(0);
+#pragma unroll
+    for (int i = 0; i < P; ++i) n2 += zz[i] * zz[i];
+    const T zn = sqrt(n2);
+    T q2 = T(0);
+    if (zn > T(0)) {
+        const T izn = T(1) / zn;
+        T qv[P];
+#pragma unroll
+        for (int i = 0; i < P; ++i) {
+            T sacc = zz[i] * izn;
+#pragma unroll
+            for (int k = 0; k < i; ++k) sacc -= L[pkl(i, k)] * qv[k];
+            qv[i] = sacc * inv[i];
+            q2 += qv[i] * qv[i];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < P; ++i) z[i] = (MS)zz[i];
+    znorm = (MS)zn;
+    w2 = (MS)q2;
+    return 0;
+}
+
+// One damped solve in working precision T with FP64 escalation for float.
+template <int P, typename T>
+__device__ __forceinline__ int damped_solve(const T (&Ms)[tri(P)], T par, const T (&g)[P], float thr,
+                                            T (&z)[P], T &znorm, T &w2, unsigned &n_esc)
+{
+    int rc = chol_solve<P, T, T>(Ms, par, g, (T)thr, z, znorm, w2);
+    if (rc == 1) {
+        ++n_esc;
+        rc = chol_solve<P, double, T>(Ms, par, g, 0.0, z, znorm, w2);
+    }
+    return rc;
+}
+
+// MINPACK/GSL lmpar in scaled coordinates (see chol_solve). On return z is
+// the accepted scaled step and par the Levenberg parameter it was solved with.
+template <int P, typename T>
+__device__ __forceinline__ void lmpar_scaled(const T (&Ms)[tri(P)], const T (&g)[P], T delta, T &par,
+                                             T (&z)[P], float thr, unsigned &n_lambda, unsigned &n_esc,
+                                             bool &singular)
+{
+    T dxnorm, w2;
+    singular = false;
+    ++n_lambda;
+    int rc = damped_solve<P, T>(Ms, T(0), g, thr, z, dxnorm, w2, n_esc);
+    bool rank_def = false;
+    if (rc != 0) {  // Newton step undefined: treat as infinitely long, no lower bound
+        rank_def = true;
+        dxnorm = (T)INFINITY;
+        w2 = T(0);
+    }
+    T fp = dxnorm - delta;
+    if (!rank_def && fp <= T(0.1) * delta) {
+        par = T(0);
+        return;
+    }
+    T par_l = (!rank_def && w2 > T(0)) ? fp / (delta * w2) : T(0);
+    T gn2 = T(0);
+#pragma unroll
+    for (int i = 0; i < P; ++i) gn2 += g[i] * g[i];
+    const T gnorm = sqrt(gn2);
+    T par_u = gnorm / delta;
+    if (par_u == T(0)) par_u = tiny_pos<T>() / (delta < T(0.1) ? delta : T(0.1));
+    T pr = par;
+    if (pr > par_u) pr = par_u;
+    else if (pr < par_l) pr = par_l;
+    if (pr == T(0)) pr = gnorm / dxnorm;
+#pragma unroll 1
+    for (int it = 1;; ++it) {
+        if (pr == T(0)) {
+            const T t = T(0.001) * par_u;
+            pr = t > tiny_pos<T>() ? t : tiny_pos<T>();
+        }
+        ++n_lambda;
+        rc = damped_solve<P, T>(Ms, pr, g, thr, z, dxnorm, w2, n_esc);
+        if (rc != 0) {
+            singular = true;
+            break;
+        }
+        const T fp_old = fp;
+        fp = dxnorm - delta;
+        if (fabs(fp) <= T(0.1) * delta) break;
+        if (par_l == T(0) && fp <= fp_old && fp_old < T(0)) break;
+        if (it == 10) break;
+        const T par_c = fp / (delta * w2);
+        if (fp > T(0)) {
+            if (pr > par_l) par_l = pr;
+        } else if (fp < T(0)) {
+            if (pr < par_u) par_u = pr;
+        }
+        pr = (par_l > pr + par_c) ? par_l : pr + par_c;
+    }
+    par = pr;
+}
+
+}  // namespace locb

@@ -1,0 +1,51 @@
+// Host-side interface of the fit kernels (used by the C ABI layer).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace locb {
+
+constexpr int kMaxHalfWidth = 16;  // LOC_MAX_HALF_WIDTH
+
+// Device scratch of one fit call. The caller provides the memory; sizes in
+// bytes come from scratch_bytes().
+struct Scratch {
+    int *cls;            // n: ROI half-width class of each candidate, -1 if not enqueued
+    int *order;          // n: enqueued candidates grouped by class
+    int *meta;           // kMetaInts: class table (see loc_fit.cu)
+    float *state;        // n * state_stride(method): solver state for the finaliser
+    unsigned long long *stats;  // 8 counters
+};
+
+constexpr int kMetaInts = 8 + 6 * (kMaxHalfWidth + 1);
+
+struct FitParams {
+    const uint16_t *frames;
+    int n_frames, n_rows, n_cols;
+    const void *cands;  // loc_candidate / Cand
+    int n_cands;
+    int method;
+    double w0, sigma;
+    int max_iter;
+    double epsabs, epsrel;
+    int precision;       // 0 fp32, 1 fp64
+    float pivot_thr;
+    int threads_per_block;
+    int blocks_per_sm;
+    int max_half_width;  // largest r present (known to the caller) or 0 = read back
+    const float *init_params;
+    float *params_out;
+    double *out;
+    uint8_t *flags;
+};
+
+int state_stride(int method);
+size_t scratch_bytes(int method, int n_cands);
+void carve_scratch(void *base, int method, int n_cands, Scratch *s);
+
+// Enqueue the whole fit on `stream`. Returns cudaSuccess or the launch error;
+// *used_smem_side receives the ROI side the solver was sized for.
+cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t stream, int *err_detail);
+
+}  // namespace locb

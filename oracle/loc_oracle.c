@@ -642,3 +642,30 @@ int oracle_find_adjacent8(const uint16_t *frame, int n_rows, int n_cols,
     free(queue);
     return nfound;
 }
+
+/* Trajectory of one fit for cross-checking the solver restatement against an
+ * independent MINPACK: after every iterate() call records the cumulative
+ * number of trial evaluations and the current point. Returns the number of
+ * records written (at most max_rec). */
+int oracle_trajectory(int method, const double *roi, int r, double x_offset, double y_offset, double w0,
+                      double sigma, const double *x0, int max_rec, int *trials, double *xs)
+{
+    const int p = n_params(method);
+    const int size = 2 * r + 1, n = size * size;
+    fit_data d = {roi, size, x_offset, y_offset, sigma, w0};
+    lmc_state st;
+    if (lmc_alloc(&st, (size_t)n, (size_t)p) != 0) return -1;
+    lmc_f_fn ff = method == 0 ? sym_f : method == 1 ? fixed_f : ell_f;
+    lmc_df_fn dff = method == 0 ? sym_df : method == 1 ? fixed_df : ell_df;
+    lmc_set(&st, ff, dff, &d, x0);
+    int k = 0;
+    while (k < max_rec) {
+        int status = lmc_iterate(&st);
+        trials[k] = (int)st.n_f_evals;
+        for (int i = 0; i < p; i++) xs[k * p + i] = st.x[i];
+        k++;
+        if (status != 0) break;
+    }
+    lmc_free(&st);
+    return k;
+}

@@ -67,6 +67,11 @@ int oracle_glrt_mask(const uint16_t *frame, int n_rows, int n_cols, double pfa,
 int oracle_find_adjacent8(const uint16_t *frame, int n_rows, int n_cols,
                           const int32_t *mask, double *out, int max_out);
 
+/* Solver trajectory of one fit (tests of the lmsder restatement): after each
+ * iterate() call, the cumulative trial evaluations and the current point. */
+int oracle_trajectory(int method, const double *roi, int r, double x_offset, double y_offset, double w0,
+                      double sigma, const double *x0, int max_rec, int *trials, double *xs);
+
 /* Instrumentation of the last oracle_fit call: sums over all candidates. */
 void oracle_last_counters(long *n_iterate_calls, long *n_f_evals, long *n_df_evals,
                           long *n_lambda_trials);

@@ -63,6 +63,9 @@ def lib():
         L.oracle_glrt_mask.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p]
         L.oracle_find_adjacent8.restype = C.c_int
         L.oracle_find_adjacent8.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+        L.oracle_trajectory.restype = C.c_int
+        L.oracle_trajectory.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double,
+                                        C.c_double, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.oracle_last_counters.restype = None
         L.oracle_last_counters.argtypes = [C.POINTER(C.c_long)] * 4
         _lib = L
@@ -134,6 +137,18 @@ def model_jacobian(method, params, w0, sigma, x_off, y_off, r, roi):
     if rc != 0:
         raise ValueError(rc)
     return f, J
+
+
+def trajectory(method, roi, r, x_off, y_off, w0, sigma, x0, max_rec=200):
+    """(cumulative trial evaluations, point) after each iterate() call."""
+    roi = np.ascontiguousarray(roi, dtype=np.float64)
+    x0 = np.ascontiguousarray(x0, dtype=np.float64)
+    p = N_PARAMS[method]
+    trials = np.zeros(max_rec, dtype=np.int32)
+    xs = np.zeros((max_rec, p))
+    k = lib().oracle_trajectory(method, roi.ctypes.data, r, x_off, y_off, w0, sigma, x0.ctypes.data, max_rec,
+                                trials.ctypes.data, xs.ctypes.data)
+    return trials[:k], xs[:k]
 
 
 def glrt_mask(frame2d, pfa, psf_width):

@@ -1,0 +1,184 @@
+"""CUDA path versus the oracle and the reference's golden outputs.
+
+Gates (from the fitting path's definition): positions within 1e-3 px of the
+FP64 oracle and >= 99.9 % agreement of accept/reject flags. Other columns
+are compared with the tolerances written next to each check.
+"""
+import numpy as np
+import pytest
+
+import localizer_b200 as L
+from localizer_b200 import synth
+from oracle import oracle as O
+from tests import _golden as G
+
+pytestmark = pytest.mark.gpu
+
+POS_TOL = 1e-3            # px, FP32 path vs FP64 oracle
+POS_FRACTION = 0.999      # fraction of jointly kept rows within POS_TOL
+FLAG_AGREEMENT = 0.999
+POS_TOL_FP64 = 1e-6       # px, FP64 GPU path vs FP64 oracle
+XCOL = {0: 3, 1: 2, 5: 4, 7: 4}
+
+
+@pytest.fixture(scope="module")
+def engine():
+    e = L.Engine(0)
+    yield e
+    e.close()
+
+
+def compare(rows, flags, ref_rows, ref_kept, method):
+    kept = flags == 0
+    agree = np.mean(kept == ref_kept) if len(kept) else 1.0
+    both = kept & ref_kept
+    xi = XCOL[method]
+    err = np.abs(rows[both, xi:xi + 2] - ref_rows[both, xi:xi + 2]).max(axis=1) if both.any() else np.zeros(0)
+    frac = np.mean(err < POS_TOL) if len(err) else 1.0
+    return agree, frac, err, both
+
+
+@pytest.mark.parametrize("name,method", list(G.all_cases()))
+def test_fp32_matches_reference_golden(engine, name, method):
+    g = G.load(name)
+    rows, flags = engine.fit_host(g["frames"], g["cands"], method, g["w0"])
+    ref_kept = g[f"kept_{method}"] == 1
+    agree, frac, err, both = compare(rows, flags, g[f"out_{method}"], ref_kept, method)
+    n = len(flags)
+    # small fixtures: at most one disagreement where 0.1 % of n is below one
+    assert np.sum((flags == 0) != ref_kept) <= max(1, int(0.001 * n)), (agree, np.nonzero((flags == 0) != ref_kept))
+    assert np.sum(err >= POS_TOL) <= max(1, int((1 - POS_FRACTION) * len(err))), np.sort(err)[-5:]
+    # edge rejects are decided before any arithmetic: exact
+    assert np.array_equal(flags == 1, np.isnan(g[f"out_{method}"][:, 1]) & (g[f"iters_{method}"] < 0))
+
+
+@pytest.mark.parametrize("name,method", list(G.all_cases()))
+def test_fp64_gpu_path_matches_oracle(engine, name, method):
+    g = G.load(name)
+    opts = L.default_options(precision=1)
+    rows, flags = engine.fit_host(g["frames"], g["cands"], method, g["w0"], options=opts)
+    out, oflags, _, _ = O.fit(g["frames"], g["cands"], method, g["w0"])
+    agree, frac, err, both = compare(rows, flags, out, oflags == 0, method)
+    assert np.sum(flags != oflags) <= 1
+    assert np.mean(err < POS_TOL_FP64) >= 0.99
+    ncol = O.REF_COLUMNS[method]
+    # iteration counts follow the FP64 oracle step for step
+    assert np.mean(rows[:, ncol] == out[:, ncol]) >= 0.98
+
+
+def _workload(name, n_frames, seed=None):
+    w = synth.scaled(synth.workloads()[name], n_frames, seed)
+    frames, em = synth.make(w)
+    cands = L.find_candidates(frames, 30.0, w.w0)
+    rng = np.random.default_rng(w.seed + 17)
+    cands["half_width"] = rng.choice(np.array(w.half_widths), size=len(cands))
+    return w, frames, cands
+
+
+@pytest.mark.parametrize("wname,method,n_frames", [("uneven", 7, 24), ("uneven", 5, 12), ("uneven", 0, 12),
+                                                   ("small", 0, 64), ("small", 1, 32), ("stress", 0, 24)])
+def test_fp32_matches_oracle_seeded(engine, wname, method, n_frames):
+    w, frames, cands = _workload(wname, n_frames)
+    rows, flags = engine.fit_host(frames, cands, method, w.w0)
+    out, oflags, _, _ = O.fit(frames, cands, method, w.w0, nthreads=8)
+    agree, frac, err, both = compare(rows, flags, out, oflags == 0, method)
+    assert agree >= FLAG_AGREEMENT or np.sum((flags == 0) != (oflags == 0)) <= 1, agree
+    assert frac >= POS_FRACTION or np.sum(err >= POS_TOL) <= 1, (frac, np.sort(err)[-5:])
+    ncol = O.REF_COLUMNS[method]
+    # widths / background / integral: relative 1e-3; uncertainties: 1e-2
+    value_cols = {0: [1, 2, 5], 1: [1, 4], 5: [1, 2, 3, 7], 7: [1, 2, 3, 7]}[method]
+    dev_cols = {0: [6, 7, 8, 9, 10], 1: [5, 6, 7, 8], 5: [11, 12, 14], 7: [11, 12, 14]}[method]
+    ok = both & (err < POS_TOL) if len(err) else both
+    sel = np.nonzero(both)[0][err < POS_TOL]
+    for cols, tol in ((value_cols, 1e-3), (dev_cols, 1e-2)):
+        a, b = rows[sel][:, cols], out[sel][:, cols]
+        rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-12)
+        assert np.mean(rel.max(axis=1) < tol) >= 0.995, (cols, np.sort(rel.max(axis=1))[-5:])
+    assert ok.sum() > 0.5 * len(cands)
+
+
+def test_device_pointer_api_matches_host_api(engine):
+    import torch
+    g = G.load("uneven")
+    frames, cands = g["frames"], g["cands"]
+    d_frames = torch.from_numpy(frames.view(np.int16)).cuda()
+    d_cands = torch.from_numpy(cands.view(np.uint8)).cuda()
+    n = len(cands)
+    ncol = L.lib().loc_output_columns(7)
+    d_out = torch.empty((n, ncol), dtype=torch.float64, device="cuda")
+    d_flags = torch.empty(n, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    engine.fit_device(d_frames.data_ptr(), frames.shape[0], frames.shape[2], frames.shape[1], d_cands.data_ptr(), n,
+                      7, g["w0"], 1.0, d_out.data_ptr(), d_flags.data_ptr(), stream,
+                      L.default_options(max_half_width=int(cands["half_width"].max())))
+    engine.sync(stream)
+    rows_h, flags_h = engine.fit_host(frames, cands, 7, g["w0"])
+    np.testing.assert_array_equal(d_flags.cpu().numpy(), flags_h)
+    np.testing.assert_array_equal(d_out.cpu().numpy(), rows_h)
+
+
+def test_edge_cases(engine):
+    g = G.load("small")
+    frames = g["frames"]
+    # empty candidate list
+    rows, flags = engine.fit_host(frames, np.zeros(0, dtype=L.CANDIDATE_DTYPE), 0, 1.3)
+    assert rows.shape == (0, 14) and flags.shape == (0,)
+    c = np.zeros(8, dtype=L.CANDIDATE_DTYPE)
+    c["x"] = [64.2, 2.0, np.nan, 64.0, 64.0, 64.0, 64.3, 64.3]
+    c["y"] = [64.7, 64.0, 64.0, 64.0, 64.0, 64.0, 64.1, 64.1]
+    c["intensity"] = 300.0
+    c["background"] = 100.0
+    c["frame"] = [0, 0, 0, 7, -1, 0, 0, 0]
+    c["half_width"] = [0, 0, 0, 0, 0, 17, 16, 3]
+    rows, flags = engine.fit_host(frames, c, 0, 1.3)
+    assert flags[1] == 1                      # edge
+    assert list(flags[2:6]) == [10, 10, 10, 10]  # NaN, frame out of range (x2), half-width above the cap
+    assert rows[1, 0] == 0 and np.isnan(rows[1, 1])
+    out, oflags, _, _ = O.fit(frames, c, 0, 1.3)
+    np.testing.assert_array_equal(flags, oflags)
+    k = flags == 0
+    np.testing.assert_allclose(rows[k, 3:5], out[k, 3:5], atol=POS_TOL)
+
+
+@pytest.mark.parametrize("method", [0, 7])
+def test_noise_weight_and_iteration_cap(engine, method):
+    g = G.load("uneven")
+    frames, cands = g["frames"], g["cands"]
+    for sigma, max_iter in ((2.5, 200), (1.0, 3)):
+        opts = L.default_options(max_iter=max_iter, precision=1)
+        rows, flags = engine.fit_host(frames, cands, method, g["w0"], sigma, options=opts)
+        out, oflags, _, _ = O.fit(frames, cands, method, g["w0"], sigma=sigma, max_iter=max_iter)
+        ncol = O.REF_COLUMNS[method]
+        assert np.mean(flags == oflags) >= 0.99
+        assert np.mean(rows[:, ncol] == out[:, ncol]) >= 0.98
+        if max_iter == 3:
+            assert rows[:, ncol].max() <= 3
+            assert np.any(rows[:, ncol + 1] == 1)
+
+
+def test_warm_start_from_converged_parameters(engine):
+    g = G.load("uneven")
+    frames, cands = g["frames"], g["cands"]
+    import torch
+    n = len(cands)
+    out, oflags, params, _ = O.fit(frames, cands, 7, g["w0"])
+    init = np.where(np.isfinite(params), params, 0).astype(np.float32)
+    d_init = torch.from_numpy(init).cuda()
+    opts = L.default_options(d_init_params=d_init.data_ptr())
+    rows, flags = engine.fit_host(frames, cands, 7, g["w0"], options=opts)
+    kept = (flags == 0) & (oflags == 0)
+    assert kept.sum() > 0.8 * n
+    assert np.median(rows[kept, 16]) <= 3
+    assert np.max(np.abs(rows[kept, 4:6] - out[kept, 4:6])) < 5e-3
+
+
+def test_deterministic_and_order_independent(engine):
+    w, frames, cands = _workload("uneven", 6, seed=99)
+    r1, f1 = engine.fit_host(frames, cands, 7, w.w0)
+    r2, f2 = engine.fit_host(frames, cands, 7, w.w0)
+    np.testing.assert_array_equal(r1, r2)
+    np.testing.assert_array_equal(f1, f2)
+    perm = np.random.default_rng(1).permutation(len(cands))
+    r3, f3 = engine.fit_host(frames, cands[perm], 7, w.w0)
+    np.testing.assert_array_equal(r3, r1[perm])
+    np.testing.assert_array_equal(f3, f1[perm])
