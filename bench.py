@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Throughput of the B200 Gaussian-PSF fit engine (fits/s) on the batched,
+uneven-ROI workload: 10,000 frames of 256 x 256 uint16, 20-400 emitters per
+frame, ellipsoidal PSFs (sigma_x, sigma_y ~ U[1, 2] px), ROI half-width per
+candidate drawn from {3, 4, 5, 6}, amplitude lognormal (median 800),
+background U[50, 200], Poisson + Gaussian read noise (sigma 2 ADU), gain 1.
+Frames are generated on the GPU from seeded emitters; candidates come from
+the GLRT + adjacent-8 finder; every candidate is fitted by the ellipsoidal
+Gaussian method (code 7) in one persistent FP32 solver launch per step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One JSON line on rank 0. A step = one fit call over every candidate of the
+stack (frames and candidates resident in HBM). `e2e` runs the same fit
+through the host-buffer C-ABI call (loc_fit_host: frame and candidate upload
+from pinned host memory, fit, row and flag download) every step. The CPU
+reference arm runs the reference's own fitter (Localization.cpp compiled
+from the reference sources into oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fits/s at ≤1e-3 px vs FP64: learned-warm-start LM vs plain LM, 1 B200"
+UNIT = "fits/s"
+METHOD = 7                 # FitPositions_EllipsoidalGaussian
+PFA = 30.0
+# algorithmic FLOPs per ROI pixel: Jacobian evaluation (model, analytic
+# Jacobian, J^T J and J^T r accumulation) and trial evaluation, and per
+# damped p x p Cholesky solve (p^3/3 + 2 p^2), for the 7-parameter model
+FLOP_J = {0: 58, 1: 46, 5: 115, 7: 115}
+FLOP_F = 12
+NPAR = {0: 5, 1: 4, 5: 7, 7: 7}
+SM_COUNT = 148
+FP32_LANES = 128
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def make_workload(n_frames: int, rank: int):
+    import torch
+
+    import localizer_b200 as L
+    from localizer_b200 import synth
+    w = synth.scaled(synth.workloads()["uneven"], n_frames, seed=1002 + 7919 * rank)
+    t0 = time.time()
+    frames_dev, em = synth.make_device(w)
+    frames_host = frames_dev.cpu().numpy().view(np.uint16)
+    t1 = time.time()
+    cands = L.find_candidates(frames_host, PFA, w.w0)
+    rng = np.random.default_rng(w.seed + 17)
+    cands["half_width"] = rng.choice(np.array(w.half_widths), size=len(cands))
+    t2 = time.time()
+    log(f"[bench] rank {rank}: {n_frames} frames rendered in {t1 - t0:.1f}s, {len(cands)} candidates found in "
+        f"{t2 - t1:.1f}s")
+    d_cands = torch.from_numpy(cands.view(np.uint8)).cuda()
+    return w, frames_dev, frames_host, cands, d_cands
+
+
+def run_reference_sample(frames_host, cands, w0, budget_s=12.0, threads=None):
+    """The reference's own fitter (oracle/_ref) on a bounded, frame-aligned
+    sample of the workload, spread over host threads. Returns
+    (fits/s, n_fits, threads, sample indices, rows, kept)."""
+    from oracle import oracle as O
+    threads = threads or os.cpu_count() or 1
+    frame_ids = cands["frame"]
+    # calibrate on one frame
+    f0 = int(frame_ids[0])
+    sel = np.nonzero(frame_ids == f0)[0]
+    t = time.time()
+    O.ref_fit(frames_host, cands[sel], METHOD, 1.5)
+    per_fit = max((time.time() - t) / max(len(sel), 1), 1e-6)
+    n_target = int(budget_s * threads / per_fit)
+    # whole frames, evenly spaced through the stack
+    counts = np.bincount(frame_ids, minlength=frames_host.shape[0])
+    n_frames = frames_host.shape[0]
+    per_frame = max(counts.mean(), 1)
+    nf = int(min(n_frames, max(threads, n_target / per_frame)))
+    chosen = np.linspace(0, n_frames - 1, nf).astype(int)
+    chosen = np.unique(chosen)
+    mask = np.isin(frame_ids, chosen)
+    idx = np.nonzero(mask)[0]
+    sub = np.ascontiguousarray(cands[idx])
+    chunks = np.array_split(np.arange(len(chosen)), threads)
+    results = [None] * len(chunks)
+
+    def work(k):
+        fr = chosen[chunks[k]]
+        m = np.isin(sub["frame"], fr)
+        results[k] = (np.nonzero(m)[0], O.ref_fit(frames_host, np.ascontiguousarray(sub[m]), METHOD, 1.5))
+
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=work, args=(k,)) for k in range(len(chunks)) if len(chunks[k])]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    dt = time.perf_counter() - t0
+    rows = np.full((len(sub), O.REF_COLUMNS[METHOD]), np.nan)
+    kept = np.zeros(len(sub), dtype=bool)
+    for r in results:
+        if r is None:
+            continue
+        ii, (out, kp, _, _) = r
+        rows[ii] = out
+        kept[ii] = kp == 1
+    return len(sub) / dt, len(sub), len(ths), idx, rows, kept
+
+
+def reference_arm(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libloc_ref.so is absent"}))
+        return 0
+    import torch
+    torch.cuda.set_device(local)
+    w, frames_dev, frames_host, cands, d_cands = make_workload(args.frames, 0)
+    vals = []
+    for step in range(args.warmup + args.steps):
+        v, n, th, _, _, _ = run_reference_sample(frames_host, cands, w.w0, budget_s=args.ref_budget)
+        if step >= args.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * len(cands) / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; GPU-rendered frames)",
+            "impl": "reference",
+            "config": {"workload": "batched uneven: 10000 frames 256x256 uint16, 20-400 emitters/frame, "
+                                   "ellipsoidal PSF, ROI half-width in {3,4,5,6}", "frames": args.frames,
+                       "candidates": int(len(cands)), "method": METHOD},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": th, "kind": "reference",
+                             "sample": f"{n} candidates (whole frames spread through the stack) per step, "
+                                       f"reference Localization.cpp FP64 + lmsder restatement, {th} threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=10000)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--ref-budget", type=float, default=12.0, help="seconds of CPU work per reference step")
+    ap.add_argument("--precision", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+
+    import localizer_b200 as L
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    w, frames_dev, frames_host, cands, d_cands = make_workload(args.frames, rank)
+    n = len(cands)
+    eng = L.Engine(local)
+    ncol = L.lib().loc_output_columns(METHOD)
+    d_out = torch.empty((n, ncol), dtype=torch.float64, device="cuda")
+    d_flags = torch.empty(n, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    opts = L.default_options(max_half_width=int(max(w.half_widths)), precision=args.precision)
+    n_frames, size = frames_dev.shape[0], frames_dev.shape[1]
+
+    def step():
+        eng.fit_device(frames_dev.data_ptr(), n_frames, size, size, d_cands.data_ptr(), n, METHOD, w.w0, 1.0,
+                       d_out.data_ptr(), d_flags.data_ptr(), stream.cuda_stream, opts)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    solver_ms, stats_last = [], None
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+            # per-stage device times of this step (events on the same stream)
+            stats_last = eng.stats()
+            solver_ms.append(stats_last["solver_ms"])
+        end.record(stream)
+        torch.cuda.synchronize()
+    elapsed_ms = start.elapsed_time(end)
+    t = torch.tensor([elapsed_ms], device="cuda")
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        tot = torch.tensor([float(n)], device="cuda")
+        torch.distributed.all_reduce(tot)
+        total_fits = tot.item() * args.steps
+    else:
+        total_fits = float(n) * args.steps
+    elapsed_ms = t.item()
+    value = total_fits / (elapsed_ms / 1e3)
+    clocks = clk.summary()
+
+    # roofline of the solver kernel: algorithmic FLOPs / kernel time vs FP32 peak
+    st = stats_last
+    p = NPAR[METHOD]
+    flops = st["pixels_j"] * FLOP_J[METHOD] + st["pixels_f"] * FLOP_F + st["lambda_solves"] * (p ** 3 / 3 + 2 * p * p)
+    k_ms = float(np.mean(solver_ms))
+    achieved = flops / (k_ms / 1e3) / 1e12
+    peak_mhz = clocks["sm_max_mhz"] or 1965.0
+    peak = SM_COUNT * FP32_LANES * 2 * peak_mhz * 1e6 / 1e12
+
+    # e2e through the host-buffer C ABI call (pinned host memory), every rank
+    import ctypes as C
+    lib = L.lib()
+    ph_frames = torch.empty(frames_host.shape, dtype=torch.int16, pin_memory=True)
+    ph_frames.numpy().view(np.uint16)[...] = frames_host
+    ph_cands = torch.empty(cands.nbytes, dtype=torch.uint8, pin_memory=True)
+    ph_cands.numpy()[...] = cands.view(np.uint8)
+    ph_out = torch.empty((n, ncol), dtype=torch.float64, pin_memory=True)
+    ph_flags = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+
+    def e2e_step():
+        rc = lib.loc_fit_host(eng.handle, C.c_void_p(ph_frames.data_ptr()), n_frames, size, size,
+                              C.c_void_p(ph_cands.data_ptr()), n, METHOD, w.w0, 1.0, C.byref(opts),
+                              C.c_void_p(ph_out.data_ptr()), C.c_void_p(ph_flags.data_ptr()))
+        if rc != 0:
+            raise RuntimeError(lib.loc_last_error().decode())
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    dstream = torch.cuda.default_stream()
+    s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s2.record(dstream)
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    e2.record(dstream)
+    torch.cuda.synchronize()
+    t2 = torch.tensor([s2.elapsed_time(e2) / args.e2e_steps], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t2, op=torch.distributed.ReduceOp.MAX)
+    e2e = {"value": total_fits / args.steps / (t2.item() / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": int(frames_host.nbytes + cands.nbytes),
+           "d2h_bytes_per_step": int(n * ncol * 8 + n)}
+    rows_e2e = ph_out.numpy().copy()
+    flags_e2e = ph_flags.numpy().copy()
+
+    # CPU reference on a bounded sample, and the accuracy of the GPU rows there
+    cpu, accuracy = None, None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        rows_gpu = d_out.cpu().numpy()
+        flags_gpu = d_flags.cpu().numpy()
+        assert np.array_equal(rows_gpu[:, :ncol - 2], rows_e2e[:, :ncol - 2], equal_nan=True)
+        assert np.array_equal(flags_gpu, flags_e2e)
+        if O.ref_available():
+            v, ns, th, idx, rrows, rkept = run_reference_sample(frames_host, cands, w.w0, budget_s=args.ref_budget)
+            cpu = {"value": v, "unit": UNIT, "cores": th, "kind": "reference",
+                   "sample": f"{ns} candidates (whole frames spread through the stack); reference "
+                             f"Localization.cpp FP64 + lmsder restatement, {th} host threads"}
+            g = rows_gpu[idx]
+            gk = flags_gpu[idx] == 0
+            both = gk & rkept
+            err = np.abs(g[both, 4:6] - rrows[both, 4:6]).max(axis=1)
+            accuracy = {"sample_fits": int(len(idx)), "flag_agreement": float(np.mean(gk == rkept)),
+                        "position_within_1e-3px": float(np.mean(err < 1e-3)) if len(err) else None,
+                        "position_max_err_px": float(err.max()) if len(err) else None,
+                        "reference": "reference fitter (FP64) on the same candidates"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == 0 else "f64",
+                "data": "synthetic (seeded emitters, GPU-rendered Poisson+read-noise frames)",
+                "config": {"workload": "batched uneven: 10000 frames 256x256 uint16, 20-400 emitters/frame, "
+                                       "ellipsoidal PSF sigma U[1,2], ROI half-width in {3,4,5,6}, method 7",
+                           "frames_per_gpu": n_frames, "candidates_per_gpu": n, "parallelism": f"dp{world}",
+                           "l2": "inputs larger than L2 (1.3 GB frames, 84 MB candidates, 300 MB rows)"},
+                "plain_lm_fits_per_s": value, "warm_start_lm_fits_per_s": None,
+                "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                             "frac": achieved / peak, "traffic": None,
+                             "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 x max SM clock); "
+                                            "no measured FP32 peak in MEASURED_PEAKS.json",
+                             "kernel": "k1_lm_fit", "kernel_ms": k_ms, "flops_per_step": flops},
+                "stats": st, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "accuracy": accuracy,
+                "gpu_launches": 5 * args.steps}
+        print(json.dumps(line))
+    eng.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

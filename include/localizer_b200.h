@@ -109,6 +109,13 @@ typedef struct loc_options {
                                   start); NULL = reference start values */
     float *d_params_out;       /* optional device array, n_cands x p floats:
                                   raw fitted parameters (absolute coordinates) */
+    float *d_diag;             /* optional device array, n_cands x 8 floats of
+                                  solver diagnostics: smallest undamped pivot
+                                  ratio, last step / stopping tolerance, FP64
+                                  pivot escalations, smallest relative margin
+                                  of a solver branch decision, 1 if the fit was
+                                  re-run in FP64, iterations and status of the
+                                  FP32 run, reserved */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */
@@ -169,7 +176,9 @@ LOC_API int loc_sync(loc_ctx *ctx, void *stream);
 
 /* Counters of the last fit call (after loc_sync): trial-point evaluations,
  * Jacobian evaluations, damped Cholesky solves, FP64 pivot escalations,
- * candidates enqueued and total solver iterations. */
+ * candidates enqueued, total solver iterations, and the device time of each
+ * stage (CUDA events on the call's stream; not recorded while the stream is
+ * being captured into a graph). */
 typedef struct loc_stats {
     uint64_t f_evals;
     uint64_t jacobian_evals;
@@ -179,6 +188,9 @@ typedef struct loc_stats {
     uint64_t iterations;
     uint64_t pixels_f;     /* sum over trial evaluations of ROI pixels */
     uint64_t pixels_j;     /* sum over Jacobian evaluations of ROI pixels */
+    float queue_ms;        /* device time of the work-queue build (-1 if not timed) */
+    float solver_ms;       /* device time of the persistent solver kernel */
+    float finalize_ms;     /* device time of the FP64 finaliser */
 } loc_stats;
 LOC_API int loc_last_stats(loc_ctx *ctx, loc_stats *stats);
 
@@ -205,6 +217,20 @@ LOC_API int loc_compact_host(const double *out, const uint8_t *flags, int n_cand
 LOC_API long loc_find_candidates_host(const uint16_t *frames, int n_frames, int n_rows,
                                       int n_cols, double pfa, double psf_width, int n_threads,
                                       loc_candidate *cands, long max_cands);
+
+/*
+ * Synthetic frames on the device (workload generation for tests and
+ * benchmarks; not part of the fit path): background + point-sampled 2D
+ * Gaussians, Poisson shot noise plus Gaussian read noise, uint16 output.
+ * d_emitters: 5 floats per emitter (x, y, amplitude, sigma_x, sigma_y),
+ * grouped by frame; d_frame_start: n_frames + 1 offsets into it;
+ * d_background: one value per frame. No reference counterpart (the
+ * reference reads camera files, source/FileIO.cpp).
+ */
+LOC_API int loc_synth_frames(uint16_t *d_frames, int n_frames, int n_rows, int n_cols,
+                             const float *d_emitters, const int *d_frame_start,
+                             const float *d_background, float read_noise, unsigned long long seed,
+                             void *stream);
 
 /*
  * Compatibility entry points with the signatures of the reference DLL

@@ -47,15 +47,17 @@ class Options(C.Structure):
     _fields_ = [("max_iter", C.c_int32), ("epsabs", C.c_double), ("epsrel", C.c_double),
                 ("precision", C.c_int32), ("pivot_threshold", C.c_float), ("threads_per_block", C.c_int32),
                 ("blocks_per_sm", C.c_int32), ("stage_u16", C.c_int32), ("max_half_width", C.c_int32),
-                ("d_init_params", C.c_void_p), ("d_params_out", C.c_void_p)]
+                ("d_init_params", C.c_void_p), ("d_params_out", C.c_void_p), ("d_diag", C.c_void_p)]
 
 
 class Stats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("f_evals", "jacobian_evals", "lambda_solves", "fp64_escalations",
-                                          "fits", "iterations", "pixels_f", "pixels_j")]
+                                          "fits", "iterations", "pixels_f", "pixels_j")] + \
+               [(n, C.c_float) for n in ("queue_ms", "solver_ms", "finalize_ms")]
 
     def as_dict(self):
-        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+        return {n: (float(getattr(self, n)) if n.endswith("_ms") else int(getattr(self, n)))
+                for n, _ in self._fields_}
 
 
 # names and prototypes of every exported entry point of include/localizer_b200.h
@@ -76,6 +78,8 @@ _PROTOS = {
     "loc_compact_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int]),
     "loc_find_candidates_host": (C.c_long, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                             C.c_int, C.c_void_p, C.c_long]),
+    "loc_synth_frames": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_float, C.c_ulonglong, C.c_void_p]),
     "LocalizerFitEmitters": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                        C.POINTER(C.c_int), C.POINTER(C.POINTER(C.c_double))]),
     "LocalizerFree": (None, [C.c_void_p]),

@@ -60,8 +60,8 @@ struct loc_ctx {
     // device copies for the host-buffer path
     DevBuf frames, cands, out, flags;
     unsigned long long *stats_dev = nullptr;  // points into scratch of the last call
-    loc_stats last{};
-    bool stats_valid = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool events_recorded = false;
 };
 
 extern "C" {
@@ -113,6 +113,12 @@ LOC_API int loc_ctx_create(loc_ctx **ctx, int device)
     loc_ctx *c = new (std::nothrow) loc_ctx();
     if (!c) return fail(LOC_E_NOMEM, "context allocation failed");
     c->device = device;
+    for (int k = 0; k < 4; ++k) {
+        if ((e = cudaEventCreate(&c->ev[k])) != cudaSuccess) {
+            delete c;
+            return cuda_fail(e, "cudaEventCreate");
+        }
+    }
     *ctx = c;
     return LOC_OK;
 }
@@ -126,6 +132,8 @@ LOC_API int loc_ctx_destroy(loc_ctx *ctx)
     ctx->cands.release();
     ctx->out.release();
     ctx->flags.release();
+    for (int k = 0; k < 4; ++k)
+        if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
     delete ctx;
     return LOC_OK;
 }
@@ -158,7 +166,7 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     if (!(o.epsrel >= 0) || !(o.epsabs >= 0)) return fail(LOC_E_INVALID, "negative tolerance");
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
-    const size_t need = locb::scratch_bytes(method, n_cands);
+    const size_t need = locb::scratch_bytes(method, n_cands, o.precision);
     e = ctx->scratch.ensure(need);
     if (e != cudaSuccess) return fail(LOC_E_NOMEM, std::string("scratch allocation: ") + cudaGetErrorString(e));
     locb::Scratch s;
@@ -183,12 +191,16 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     p.max_half_width = o.max_half_width;
     p.init_params = o.d_init_params;
     p.params_out = o.d_params_out;
+    p.diag = o.d_diag;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing((cudaStream_t)stream, &cap);
+    for (int k = 0; k < 4; ++k) p.ev[k] = cap == cudaStreamCaptureStatusNone ? ctx->ev[k] : nullptr;
+    ctx->events_recorded = cap == cudaStreamCaptureStatusNone;
     p.out = d_out;
     p.flags = d_flags;
     int detail = 0;
     e = locb::enqueue_fit(p, s, (cudaStream_t)stream, &detail);
     ctx->stats_dev = s.stats;
-    ctx->stats_valid = false;
     if (e != cudaSuccess) {
         if (detail == 1) return fail(LOC_E_UNSUPPORTED, "ROI too large for shared memory");
         return cuda_fail(e, "fit launch");
@@ -222,6 +234,12 @@ LOC_API int loc_last_stats(loc_ctx *ctx, loc_stats *st)
     st->iterations = v[5];
     st->pixels_f = v[6];
     st->pixels_j = v[7];
+    st->queue_ms = st->solver_ms = st->finalize_ms = -1.0f;
+    if (ctx->events_recorded && cudaEventSynchronize(ctx->ev[3]) == cudaSuccess) {
+        cudaEventElapsedTime(&st->queue_ms, ctx->ev[0], ctx->ev[1]);
+        cudaEventElapsedTime(&st->solver_ms, ctx->ev[1], ctx->ev[2]);
+        cudaEventElapsedTime(&st->finalize_ms, ctx->ev[2], ctx->ev[3]);
+    }
     return LOC_OK;
 }
 

@@ -40,9 +40,10 @@ __host__ __device__ constexpr int pku(int P, int i, int j) { return i * P - i * 
 // packed lower triangle (row-major, j <= i)
 __host__ __device__ constexpr int pkl(int i, int j) { return i * (i + 1) / 2 + j; }
 
-// Per-candidate fit state handed from the solver kernel to the finaliser.
-// Floats: [0,P) parameters (ROI-local positions), [P, P+NT) scaled J^T J,
-// then fnorm, iterations, status, x_off, y_off (ints stored bitwise).
+// Per-candidate fit state handed from the solver kernel to the finaliser, in
+// the solver's precision: [0,P) parameters (ROI-local positions), [P, P+NT)
+// scaled J^T J, then fnorm, iterations, status, x_off, y_off (small integers,
+// exact in either precision).
 template <int P> struct StateLayout {
     static constexpr int NT = tri(P);
     static constexpr int FNORM = P + NT;
@@ -50,7 +51,11 @@ template <int P> struct StateLayout {
     static constexpr int STATUS = FNORM + 2;
     static constexpr int XOFF = FNORM + 3;
     static constexpr int YOFF = FNORM + 4;
-    static constexpr int STRIDE = ((FNORM + 5) + 3) / 4 * 4;
+    static constexpr int MINPIV = FNORM + 5;   // smallest undamped pivot ratio over the fit
+    static constexpr int LASTR = FNORM + 6;    // last step / test_delta tolerance (max over parameters)
+    static constexpr int NESC = FNORM + 7;     // FP64 pivot escalations in the fit
+    static constexpr int MARGIN = FNORM + 8;   // smallest relative distance of a branch decision to its threshold
+    static constexpr int STRIDE = ((FNORM + 9) + 3) / 4 * 4;
 };
 
 // Reject codes and termination codes (public header LOC_FLAG_*, LOC_TERM_*).
@@ -113,28 +118,68 @@ __device__ __forceinline__ float load_px<float, float>(const float *roi, int k, 
 template <>
 __device__ __forceinline__ double load_px<double, float>(const float *roi, int k, int ld) { return (double)roi[k * ld]; }
 
+// Accurate change of |r|^2 between the current point th and the evaluated
+// point te = th + dth. The actual-reduction ratio of the trust-region test
+// needs fnorm(te)^2 - fnorm(th)^2 to a precision that an FP32 model value
+// (~600 photons, 24-bit mantissa) cannot give once steps shrink below about
+// 1e-3 px. The pass therefore also forms, per pixel, the model difference
+//   delta = m(te) - m(th) = e' (dA - A expm1(q - q')) + db
+// from the exponent difference q - q', which is written analytically in the
+// parameter step (no cancellation), and accumulates
+//   dchi = sum delta (2 r' - delta) = |r(te)|^2 - |r(th)|^2.
+// expm1 is a degree-6 series, exact to FP32 for |q - q'| < 0.25 (truncation
+// below 5e-8 relative); dqmax reports the largest |q - q'| so the caller can
+// fall back to the direct difference for larger steps, whose reduction is
+// large enough for FP32 to resolve directly.
+template <typename T>
+__device__ __forceinline__ T expm1_series(T y)
+{
+    T p = fma(y, T(1.0 / 720.0), T(1.0 / 120.0));
+    p = fma(y, p, T(1.0 / 24.0));
+    p = fma(y, p, T(1.0 / 6.0));
+    p = fma(y, p, T(0.5));
+    p = fma(y, p, T(1));
+    return y * p;
+}
+
 // S > 0: compile-time ROI side (rows fully unrolled); S == 0: runtime side s_rt.
 template <int S, typename T>
-__device__ __forceinline__ void pass_sym(const float *__restrict__ roi, int ld, int s_rt,
-                                         const T (&th)[5], T (&acc)[14], T (&vv)[5], T &chi2)
+__device__ __forceinline__ void pass_sym(const float *__restrict__ roi, int ld, int s_rt, const T (&th)[5],
+                                         const T (&dth)[5], T (&acc)[14], T (&vv)[5], T &chi2, T &dchi, T &dqmax)
 {
     const int s = S > 0 ? S : s_rt;
     const T A = th[0], w = th[1], x0 = th[2], y0 = th[3], b = th[4];
+    const T dA = dth[0], dw = dth[1], dxs = dth[2], dys = dth[3], db = dth[4];
+    const T A0 = A - dA, w0c = w - dw;                         // current point
     const T w2i = T(1) / (w * w);
     const T c1 = -T(0.5) * w2i * (T)Expo<T>::scale;
     const T ka_x = A * w2i;                                   // dfdx0 = u e A / w^2
     const T ka_r = ka_x / (w * T(1.4142135623730950488));      // dfdr = d2 e A / (sqrt2 w^3)
+    // exponent q = -c d2, c = 1/(2 w^2); q' - q = -(d2' (c' - c) + c (d2' - d2))
+    const T cc = T(0.5) / (w0c * w0c);
+    const T cpr = T(0.5) * w2i;
+    const T dc = -T(2) * dw * (T(2) * w0c + dw) * cc * cpr;   // c' - c
+    const T m2dx = -T(2) * dxs;
 #pragma unroll
     for (int k = 0; k < 14; ++k) acc[k] = T(0);
 #pragma unroll
     for (int k = 0; k < 5; ++k) vv[k] = T(0);
     chi2 = T(0);
-    auto body = [&](int i, T wy, T wy2, const float *row) {
+    dchi = T(0);
+    dqmax = T(0);
+    auto body = [&](int i, T wy, T wy2, T krow, const float *row) {
         const T u = (T)i - x0;
         const T d2 = fma(u, u, wy2);
         const T e = Expo<T>::ex(d2 * c1);
         const T dat = load_px<T, float>(row, i, ld);
         const T r = fma(A, e, b - dat);
+        // accurate |r|^2 change
+        const T dd = fma(m2dx, u, krow);                      // d2' - d2
+        const T ydq = fma(d2, dc, cc * dd);                   // q - q'
+        dqmax = fmax(dqmax, fabs(ydq));
+        const T del = fma(e, fma(-A0, expm1_series(ydq), dA), db);
+        dchi = fma(del, fma(T(2), r, -del), dchi);
+        // Jacobian and normal equations at the evaluated point
         const T jr = d2 * (e * ka_r);
         const T ex = e * ka_x;
         const T jx = u * ex, jy = wy * ex;
@@ -152,37 +197,48 @@ __device__ __forceinline__ void pass_sym(const float *__restrict__ roi, int ld, 
     for (int j = 0; j < s; ++j) {
         const T wy = (T)j - y0;
         const T wy2 = wy * wy;
+        const T krow = -dxs * dxs - dys * (T(2) * wy + dys);  // (d2' - d2) minus its u term
         const float *row = roi + j * s * ld;
         if (S > 0) {
 #pragma unroll
-            for (int i = 0; i < (S > 0 ? S : 1); ++i) body(i, wy, wy2, row);
+            for (int i = 0; i < (S > 0 ? S : 1); ++i) body(i, wy, wy2, krow, row);
         } else {
 #pragma unroll 1
-            for (int i = 0; i < s; ++i) body(i, wy, wy2, row);
+            for (int i = 0; i < s; ++i) body(i, wy, wy2, krow, row);
         }
     }
 }
 
 template <int S, typename T>
-__device__ __forceinline__ void pass_fixed(const float *__restrict__ roi, int ld, int s_rt, T w0,
-                                           const T (&th)[4], T (&acc)[9], T (&vv)[4], T &chi2)
+__device__ __forceinline__ void pass_fixed(const float *__restrict__ roi, int ld, int s_rt, T w0, const T (&th)[4],
+                                           const T (&dth)[4], T (&acc)[9], T (&vv)[4], T &chi2, T &dchi, T &dqmax)
 {
     const int s = S > 0 ? S : s_rt;
     const T A = th[0], x0 = th[1], y0 = th[2], b = th[3];
+    const T dA = dth[0], dxs = dth[1], dys = dth[2], db = dth[3];
+    const T A0 = A - dA;
     const T w2i = T(1) / (w0 * w0);
     const T c1 = -T(0.5) * w2i * (T)Expo<T>::scale;
     const T ka_x = A * w2i;
+    const T cc = T(0.5) * w2i;
+    const T m2dx = -T(2) * dxs;
 #pragma unroll
     for (int k = 0; k < 9; ++k) acc[k] = T(0);
 #pragma unroll
     for (int k = 0; k < 4; ++k) vv[k] = T(0);
     chi2 = T(0);
-    auto body = [&](int i, T wy, T wy2, const float *row) {
+    dchi = T(0);
+    dqmax = T(0);
+    auto body = [&](int i, T wy, T wy2, T krow, const float *row) {
         const T u = (T)i - x0;
         const T d2 = fma(u, u, wy2);
         const T e = Expo<T>::ex(d2 * c1);
         const T dat = load_px<T, float>(row, i, ld);
         const T r = fma(A, e, b - dat);
+        const T ydq = cc * fma(m2dx, u, krow);                // q - q' = c (d2' - d2)
+        dqmax = fmax(dqmax, fabs(ydq));
+        const T del = fma(e, fma(-A0, expm1_series(ydq), dA), db);
+        dchi = fma(del, fma(T(2), r, -del), dchi);
         const T ex = e * ka_x;
         const T jx = u * ex, jy = wy * ex;
         acc[0] = fma(e, e, acc[0]); acc[1] = fma(e, jx, acc[1]); acc[2] = fma(e, jy, acc[2]); acc[3] += e;
@@ -195,23 +251,26 @@ __device__ __forceinline__ void pass_fixed(const float *__restrict__ roi, int ld
     for (int j = 0; j < s; ++j) {
         const T wy = (T)j - y0;
         const T wy2 = wy * wy;
+        const T krow = -dxs * dxs - dys * (T(2) * wy + dys);
         const float *row = roi + j * s * ld;
         if (S > 0) {
 #pragma unroll
-            for (int i = 0; i < (S > 0 ? S : 1); ++i) body(i, wy, wy2, row);
+            for (int i = 0; i < (S > 0 ? S : 1); ++i) body(i, wy, wy2, krow, row);
         } else {
 #pragma unroll 1
-            for (int i = 0; i < s; ++i) body(i, wy, wy2, row);
+            for (int i = 0; i < s; ++i) body(i, wy, wy2, krow, row);
         }
     }
 }
 
 template <int S, typename T>
-__device__ __forceinline__ void pass_ell(const float *__restrict__ roi, int ld, int s_rt,
-                                         const T (&th)[7], T (&acc)[27], T (&vv)[7], T &chi2)
+__device__ __forceinline__ void pass_ell(const float *__restrict__ roi, int ld, int s_rt, const T (&th)[7],
+                                         const T (&dth)[7], T (&acc)[27], T (&vv)[7], T &chi2, T &dchi, T &dqmax)
 {
     const int s = S > 0 ? S : s_rt;
     const T A = th[0], sx = th[1], sy = th[2], x0 = th[3], y0 = th[4], rho = th[5], b = th[6];
+    const T dA = dth[0], dsx = dth[1], dsy = dth[2], dxs = dth[3], dys = dth[4], drho = dth[5], db = dth[6];
+    const T A0 = A - dA, sx0 = sx - dsx, sy0 = sy - dsy, rho0 = rho - drho;
     const T isx = T(1) / sx, isy = T(1) / sy;
     const T a = isx * isx, c = isy * isy, bb = isx * isy;
     const T rb = rho * bb;
@@ -221,19 +280,39 @@ __device__ __forceinline__ void pass_ell(const float *__restrict__ roi, int ld, 
     const T ABK = AK * bb;
     const T rk = rho * k;
     const T tr = T(2) * rho;
+    // current-point coefficients and their exact differences to the evaluated point
+    const T isx0 = T(1) / sx0, isy0 = T(1) / sy0;
+    const T a0 = isx0 * isx0, c0 = isy0 * isy0, bb0 = isx0 * isy0;
+    const T k0 = T(1) / (T(1) - rho0 * rho0);
+    const T da = -dsx * (T(2) * sx0 + dsx) * a0 * a;          // a' - a
+    const T dcq = -dsy * (T(2) * sy0 + dsy) * c0 * c;         // c' - c
+    const T dbb = -(dsx * sy0 + sx * dsy) * bb0 * bb;          // bb' - bb
+    const T drb = drho * bb + rho0 * dbb;                      // rb' - rb
+    const T dk = drho * (T(2) * rho0 + drho) * k0 * k;         // k' - k
+    const T rb0 = rho0 * bb0;
+    const T hk = -T(0.5) * k, hdk = -T(0.5) * dk;
+    const T dx2 = dxs * dxs;
 #pragma unroll
     for (int q = 0; q < 27; ++q) acc[q] = T(0);
 #pragma unroll
     for (int q = 0; q < 7; ++q) vv[q] = T(0);
     chi2 = T(0);
-    auto body = [&](int i, T wy, T wy2, T wc, T wrb, const float *row) {
+    dchi = T(0);
+    dqmax = T(0);
+    auto body = [&](int i, T wy, T wy2, T wc, T wrb, T brow, T crow, const float *row) {
         const T u = (T)i - x0;
         const T P1 = fma(u, a, -wrb);            // u/sx^2 - rho w/(sx sy)
         const T P2 = fma(-rb, u, wc);            // w/sy^2 - rho u/(sx sy)
-        const T q = fma(u, P1, wy * P2);         // the quadratic form
+        const T q = fma(u, P1, wy * P2);         // the quadratic form Q'
         const T e = Expo<T>::ex(q * cexp);
         const T dat = load_px<T, float>(row, i, ld);
         const T r = fma(A, e, b - dat);
+        // q' - q = -(k' Q' - k Q)/2 with Q' - Q a quadratic in u (per-row coefficients)
+        const T dQ = fma(fma(da, u, brow), u, crow);
+        const T ydq = -fma(hk, dQ, hdk * (q - dQ));           // q - q'
+        dqmax = fmax(dqmax, fabs(ydq));
+        const T del = fma(e, fma(-A0, expm1_series(ydq), dA), db);
+        dchi = fma(del, fma(T(2), r, -del), dchi);
         const T ek = e * AK;
         const T jx = ek * P1, jy = ek * P2;      // dfdx0, dfdy0
         const T jsx = (jx * u) * isx;            // dfdsigmaX
@@ -263,13 +342,18 @@ __device__ __forceinline__ void pass_ell(const float *__restrict__ roi, int ld, 
         const T wy2 = wy * wy;
         const T wc = wy * c;
         const T wrb = wy * rb;
+        // Q' - Q = da u^2 + brow u + crow, u and w at the evaluated point
+        const T wcur = wy + dys;
+        const T brow = T(2) * (dxs * (da - a) - drb * wy + rb0 * dys);
+        const T crow = (da - a) * dx2 - c * dys * (T(2) * wy + dys) + dcq * wcur * wcur +
+                       T(2) * rb0 * dxs * wcur;
         const float *row = roi + j * s * ld;
         if (S > 0) {
 #pragma unroll
-            for (int i = 0; i < (S > 0 ? S : 1); ++i) body(i, wy, wy2, wc, wrb, row);
+            for (int i = 0; i < (S > 0 ? S : 1); ++i) body(i, wy, wy2, wc, wrb, brow, crow, row);
         } else {
 #pragma unroll 1
-            for (int i = 0; i < s; ++i) body(i, wy, wy2, wc, wrb, row);
+            for (int i = 0; i < s; ++i) body(i, wy, wy2, wc, wrb, brow, crow, row);
         }
     }
 }
@@ -278,23 +362,30 @@ __device__ __forceinline__ void pass_ell(const float *__restrict__ roi, int ld, 
 // Damped solve in D-scaled coordinates. With M = D^-1 J^T J D^-1 and
 // g = D^-1 J^T f, the lmpar step x (J x ~ f, reference step dx = -x) is
 // D x = z with (M + par I) z = g. Returns z, |z| and |L^-1 z|^2 / |z|^2
-// (the quantity MINPACK's lmpar forms as |w|^2 through R or S).
+// (the quantity MINPACK's lmpar forms as |w|^2 through R or S), and the
+// smallest pivot ratio d_k / (M_kk + par) met in the factorisation.
 // Result codes: 0 ok, 1 an FP32 pivot fell below thr * diagonal (redo in
 // FP64), 2 not positive definite (in the precision T).
 // ---------------------------------------------------------------------------
 template <int P, typename T, typename MS>
 __device__ __forceinline__ int chol_solve(const MS (&Ms)[tri(P)], MS par, const MS (&g)[P], T thr,
-                                          MS (&z)[P], MS &znorm, MS &w2)
+                                          MS (&z)[P], MS &znorm, MS &w2, MS &minpiv)
 {
     T L[tri(P)];
     T inv[P];
+    T mp = T(1);
 #pragma unroll
     for (int j = 0; j < P; ++j) {
         const T djj = (T)Ms[pku(P, j, j)] + (T)par;
         T d = djj;
 #pragma unroll
         for (int k = 0; k < j; ++k) d -= L[pkl(j, k)] * L[pkl(j, k)];
-        if (!(d > thr * djj)) return thr > T(0) ? 1 : 2;
+        const T ratio = d / djj;
+        mp = ratio < mp ? ratio : mp;
+        if (!(d > thr * djj)) {
+            minpiv = (MS)mp;
+            return thr > T(0) ? 1 : 2;
+        }
         const T l = sqrt(d);
         inv[j] = T(1) / l;
         L[pkl(j, j)] = l;
@@ -306,6 +397,7 @@ __device__ __forceinline__ int chol_solve(const MS (&Ms)[tri(P)], MS par, const 
             L[pkl(i, j)] = sacc * inv[j];
         }
     }
+    minpiv = (MS)mp;
     T y[P];
 #pragma unroll
     for (int i = 0; i < P; ++i) {
@@ -349,34 +441,47 @@ __device__ __forceinline__ int chol_solve(const MS (&Ms)[tri(P)], MS par, const 
 // One damped solve in working precision T with FP64 escalation for float.
 template <int P, typename T>
 __device__ __forceinline__ int damped_solve(const T (&Ms)[tri(P)], T par, const T (&g)[P], float thr,
-                                            T (&z)[P], T &znorm, T &w2, unsigned &n_esc)
+                                            T (&z)[P], T &znorm, T &w2, T &minpiv, unsigned &n_esc)
 {
-    int rc = chol_solve<P, T, T>(Ms, par, g, (T)thr, z, znorm, w2);
+    int rc = chol_solve<P, T, T>(Ms, par, g, (T)thr, z, znorm, w2, minpiv);
     if (rc == 1) {
         ++n_esc;
-        rc = chol_solve<P, double, T>(Ms, par, g, 0.0, z, znorm, w2);
+        T mp2;
+        rc = chol_solve<P, double, T>(Ms, par, g, 0.0, z, znorm, w2, mp2);
     }
     return rc;
 }
 
 // MINPACK/GSL lmpar in scaled coordinates (see chol_solve). On return z is
-// the accepted scaled step and par the Levenberg parameter it was solved with.
+// the accepted scaled step and par the Levenberg parameter it was solved
+// with; newton_piv is the smallest pivot ratio of the undamped factorisation
+// (a conditioning measure of the scaled normal matrix). A damped system that
+// is not positive definite (possible only when rounding has made the
+// accumulated J^T J indefinite) raises par until it factorises.
+//
+// margin receives the smallest distance, relative to delta, between a
+// quantity and the threshold of a branch it decided (the Newton acceptance
+// fp <= 0.1 delta, the |fp| <= 0.1 delta stop, the fp <= fp_old stop): a
+// small margin means a rounding difference could have taken the other branch.
 template <int P, typename T>
 __device__ __forceinline__ void lmpar_scaled(const T (&Ms)[tri(P)], const T (&g)[P], T delta, T &par,
                                              T (&z)[P], float thr, unsigned &n_lambda, unsigned &n_esc,
-                                             bool &singular)
+                                             bool &singular, T &newton_piv, T &margin)
 {
-    T dxnorm, w2;
+    const T idelta = T(1) / delta;
+    T dxnorm, w2, mp;
     singular = false;
     ++n_lambda;
-    int rc = damped_solve<P, T>(Ms, T(0), g, thr, z, dxnorm, w2, n_esc);
+    int rc = damped_solve<P, T>(Ms, T(0), g, thr, z, dxnorm, w2, newton_piv, n_esc);
     bool rank_def = false;
     if (rc != 0) {  // Newton step undefined: treat as infinitely long, no lower bound
         rank_def = true;
         dxnorm = (T)INFINITY;
         w2 = T(0);
+        newton_piv = T(0);
     }
     T fp = dxnorm - delta;
+    if (!rank_def) margin = fmin(margin, fabs(fp - T(0.1) * delta) * idelta);
     if (!rank_def && fp <= T(0.1) * delta) {
         par = T(0);
         return;
@@ -392,6 +497,7 @@ __device__ __forceinline__ void lmpar_scaled(const T (&Ms)[tri(P)], const T (&g)
     if (pr > par_u) pr = par_u;
     else if (pr < par_l) pr = par_l;
     if (pr == T(0)) pr = gnorm / dxnorm;
+    int fails = 0;
 #pragma unroll 1
     for (int it = 1;; ++it) {
         if (pr == T(0)) {
@@ -399,14 +505,22 @@ __device__ __forceinline__ void lmpar_scaled(const T (&Ms)[tri(P)], const T (&g)
             pr = t > tiny_pos<T>() ? t : tiny_pos<T>();
         }
         ++n_lambda;
-        rc = damped_solve<P, T>(Ms, pr, g, thr, z, dxnorm, w2, n_esc);
+        rc = damped_solve<P, T>(Ms, pr, g, thr, z, dxnorm, w2, mp, n_esc);
         if (rc != 0) {
-            singular = true;
-            break;
+            // the unit-diagonal scaled matrix plus a larger shift factorises
+            if (++fails > 16) {
+                singular = true;
+                break;
+            }
+            pr = pr * T(4) > T(1e-6) ? pr * T(4) : T(1e-6);
+            --it;
+            continue;
         }
         const T fp_old = fp;
         fp = dxnorm - delta;
+        margin = fmin(margin, fabs(fabs(fp) - T(0.1) * delta) * idelta);
         if (fabs(fp) <= T(0.1) * delta) break;
+        if (par_l == T(0) && fp_old < T(0)) margin = fmin(margin, fabs(fp - fp_old) * idelta);
         if (par_l == T(0) && fp <= fp_old && fp_old < T(0)) break;
         if (it == 10) break;
         const T par_c = fp / (delta * w2);

@@ -134,8 +134,8 @@ struct K1Args {
     const Cand *cands;
     const int *order;
     int *meta;
-    float *state;
-    int state_stride;
+    void *state;
+    int state_stride;   // elements of the solver's precision per candidate
     float w0;
     float inv_s2, inv_abs_s;
     double inv_s2_d, inv_abs_s_d;
@@ -148,24 +148,25 @@ struct K1Args {
 
 template <int METHOD, int S, typename T> struct Pass;
 template <int S, typename T> struct Pass<0, S, T> {
-    __device__ __forceinline__ static void run(const float *roi, int ld, int s, T, const T (&te)[5], T (&acc)[14],
-                                               T (&vv)[5], T &chi2)
+    __device__ __forceinline__ static void run(const float *roi, int ld, int s, T, const T (&te)[5], const T (&dt)[5],
+                                               T (&acc)[14], T (&vv)[5], T &chi2, T &dchi, T &dqmax)
     {
-        pass_sym<S, T>(roi, ld, s, te, acc, vv, chi2);
+        pass_sym<S, T>(roi, ld, s, te, dt, acc, vv, chi2, dchi, dqmax);
     }
 };
 template <int S, typename T> struct Pass<1, S, T> {
-    __device__ __forceinline__ static void run(const float *roi, int ld, int s, T w0, const T (&te)[4], T (&acc)[9],
-                                               T (&vv)[4], T &chi2)
+    __device__ __forceinline__ static void run(const float *roi, int ld, int s, T w0, const T (&te)[4],
+                                               const T (&dt)[4], T (&acc)[9], T (&vv)[4], T &chi2, T &dchi,
+                                               T &dqmax)
     {
-        pass_fixed<S, T>(roi, ld, s, w0, te, acc, vv, chi2);
+        pass_fixed<S, T>(roi, ld, s, w0, te, dt, acc, vv, chi2, dchi, dqmax);
     }
 };
 template <int S, typename T> struct Pass<7, S, T> {
-    __device__ __forceinline__ static void run(const float *roi, int ld, int s, T, const T (&te)[7], T (&acc)[27],
-                                               T (&vv)[7], T &chi2)
+    __device__ __forceinline__ static void run(const float *roi, int ld, int s, T, const T (&te)[7], const T (&dt)[7],
+                                               T (&acc)[27], T (&vv)[7], T &chi2, T &dchi, T &dqmax)
     {
-        pass_ell<S, T>(roi, ld, s, te, acc, vv, chi2);
+        pass_ell<S, T>(roi, ld, s, te, dt, acc, vv, chi2, dchi, dqmax);
     }
 };
 
@@ -195,6 +196,9 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
     T th[P], A[NT], v[P], D[P], dx[P], te[P];
     T fnorm = 0, delta = 0, par = 0, xnorm = 0, jdx2 = 0, pnorm = 0;
     int phase = 0, it_state = 0, iterations = 0, trial = 0, cidx = -1, xo = 0, yo = 0;
+    T minpiv_fit = T(1);
+    T margin_fit = T(1e30);
+    unsigned esc_fit = 0;
     bool exhausted = false;
 #pragma unroll
     for (int k = 0; k < P; ++k) th[k] = v[k] = D[k] = dx[k] = te[k] = T(0);
@@ -205,27 +209,42 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
         return k == IX ? t[k] + (T)xo : (k == IX + 1 ? t[k] + (T)yo : t[k]);
     };
     auto finish = [&](int status) {
-        float *o = a.state + (size_t)cidx * a.state_stride;
+        T *o = (T *)a.state + (size_t)cidx * a.state_stride;
 #pragma unroll
-        for (int k = 0; k < P; ++k) o[k] = (float)th[k];
+        for (int k = 0; k < P; ++k) o[k] = th[k];
 #pragma unroll
-        for (int k = 0; k < NT; ++k) o[P + k] = (float)A[k];
-        o[SL::FNORM] = (float)fnorm;
-        o[SL::ITERS] = __int_as_float(iterations);
-        o[SL::STATUS] = __int_as_float(status);
-        o[SL::XOFF] = __int_as_float(xo);
-        o[SL::YOFF] = __int_as_float(yo);
+        for (int k = 0; k < NT; ++k) o[P + k] = A[k];
+        o[SL::FNORM] = fnorm;
+        o[SL::ITERS] = (T)iterations;
+        o[SL::STATUS] = (T)status;
+        o[SL::XOFF] = (T)xo;
+        o[SL::YOFF] = (T)yo;
+        T lastr = T(0);
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            const T tol = (T)a.epsabs + (T)a.epsrel * fabs(theta_abs(k, th));
+            const T q = fabs(dx[k]) / tol;
+            lastr = q > lastr ? q : lastr;
+        }
+        o[SL::MINPIV] = minpiv_fit;
+        o[SL::LASTR] = lastr;
+        o[SL::NESC] = (T)esc_fit;
+        o[SL::MARGIN] = margin_fit;
         st[ST_FITS] += 1;
         st[ST_ITERS] += iterations;
         phase = 0;
     };
     auto test_delta = [&]() -> bool {
         bool ok = true;
+        T worst = T(0);
 #pragma unroll
         for (int k = 0; k < P; ++k) {
             const T tol = (T)a.epsabs + (T)a.epsrel * fabs(theta_abs(k, th));
             ok = ok && (fabs(dx[k]) < tol);
+            const T q = fabs(dx[k]) / tol;
+            worst = q > worst ? q : worst;
         }
+        margin_fit = fmin(margin_fit, fabs(worst - T(1)));
         return ok;
     };
     auto start_iteration = [&]() {
@@ -264,6 +283,9 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
                 yo = (int)floor(cd.y - (double)r);
                 fr = cd.frame;
                 cidx = my;
+                minpiv_fit = T(1);
+                margin_fit = T(1e30);
+                esc_fit = 0;
                 if (a.init_params) {
                     const float *ip = a.init_params + (size_t)my * P;
 #pragma unroll
@@ -323,9 +345,12 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
                 for (int j = i; j < P; ++j) Ms[pku(P, i, j)] = A[pku(P, i, j)] * invD[i] * invD[j];
             unsigned nl = 0, ne = 0;
             bool sing = false;
-            lmpar_scaled<P, T>(Ms, g, delta, par, z, a.pivot_thr, nl, ne, sing);
+            T npiv;
+            lmpar_scaled<P, T>(Ms, g, delta, par, z, a.pivot_thr, nl, ne, sing, npiv, margin_fit);
             st[ST_LAMBDA] += nl;
             st[ST_ESC] += ne;
+            esc_fit += ne;
+            minpiv_fit = npiv < minpiv_fit ? npiv : minpiv_fit;
             if (sing) {
                 finish(T_SINGULAR);
             } else {
@@ -354,9 +379,12 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
         }
 
         // ---- the pass: model, Jacobian and normal equations at te ----
-        T acc[NT - 1], vv[P], chi2;
+        T acc[NT - 1], vv[P], chi2, dchi, dqmax;
         if (do_pass) {
-            Pass<METHOD, S, T>::run(myroi, ld, s, w0, te, acc, vv, chi2);
+            T dt[P];
+#pragma unroll
+            for (int k = 0; k < P; ++k) dt[k] = phase == 2 ? dx[k] : T(0);
+            Pass<METHOD, S, T>::run(myroi, ld, s, w0, te, dt, acc, vv, chi2, dchi, dqmax);
             if (phase == 1) {
                 st[ST_J] += 1;
                 st[ST_PIXJ] += npx;
@@ -395,8 +423,13 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
             } else {
                 T actred = T(-1);
                 if (T(0.1) * fn1 < fnorm) {
-                    const T u = fn1 / fnorm;
-                    actred = T(1) - u * u;
+                    if (dqmax < T(0.25)) {
+                        // accurate |f|^2 change from the per-pixel model differences
+                        actred = -(dchi * inv_s2) / (fnorm * fnorm);
+                    } else {
+                        const T u = fn1 / fnorm;
+                        actred = T(1) - u * u;
+                    }
                 }
                 const T if2 = T(1) / (fnorm * fnorm);
                 const T t1s = jdx2 * if2;
@@ -404,6 +437,8 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
                 const T prered = t1s + T(2) * t2s;
                 const T dirder = -(t1s + t2s);
                 const T ratio = prered > T(0) ? actred / prered : T(0);
+                margin_fit = fmin(margin_fit, fmin(fabs(ratio - T(0.25)), fmin(fabs(ratio - T(0.75)),
+                                                                              fabs(ratio - T(1e-4)))));
                 if (ratio > T(0.25)) {
                     if (par == T(0) || ratio >= T(0.75)) {
                         delta = pnorm / T(0.5);
@@ -506,12 +541,13 @@ struct K2Args {
     int method;
     double w0;
     int r_default;
-    const float *state;
+    const void *state;
     int state_stride;
     int ncol_total;
     double *out;
     uint8_t *flags;
     float *params_out;
+    float *diag;
 };
 
 // Symmetric 2x2 eigen-decomposition with ascending eigenvalues (the
@@ -579,7 +615,7 @@ __device__ bool inverse_diagonal(const double (&A)[tri(P)], double (&cd)[P])
     return true;
 }
 
-template <int METHOD>
+template <int METHOD, typename ST>
 __global__ void k2_finalize(K2Args a)
 {
     constexpr int P = Traits<METHOD == 5 ? 7 : METHOD>::P;
@@ -589,10 +625,10 @@ __global__ void k2_finalize(K2Args a)
     if (i >= a.n) return;
     if (a.flags[i] != F_PENDING) return;
     const Cand cd = a.cands[i];
-    const float *s = a.state + (size_t)i * a.state_stride;
-    const int iterations = __float_as_int(s[SL::ITERS]);
-    const int status = __float_as_int(s[SL::STATUS]);
-    const int xo = __float_as_int(s[SL::XOFF]), yo = __float_as_int(s[SL::YOFF]);
+    const ST *s = (const ST *)a.state + (size_t)i * a.state_stride;
+    const int iterations = (int)s[SL::ITERS];
+    const int status = (int)s[SL::STATUS];
+    const int xo = (int)s[SL::XOFF], yo = (int)s[SL::YOFF];
     const int r = cd.half_width > 0 ? cd.half_width : a.r_default;
     const int xm = xo + 2 * r, ym = yo + 2 * r;
     const double w0 = a.w0;
@@ -617,6 +653,17 @@ __global__ void k2_finalize(K2Args a)
     if (a.params_out) {
 #pragma unroll
         for (int k = 0; k < P; ++k) a.params_out[(size_t)i * P + k] = (float)x[k];
+    }
+    if (a.diag) {
+        float *dg = a.diag + (size_t)i * 8;
+        dg[0] = (float)s[SL::MINPIV];
+        dg[1] = (float)s[SL::LASTR];
+        dg[2] = (float)s[SL::NESC];
+        dg[3] = (float)s[SL::MARGIN];
+        dg[4] = 0.0f;
+        dg[5] = (float)iterations;
+        dg[6] = (float)status;
+        dg[7] = 0.0f;
     }
     uint8_t flag = F_KEPT;
     if (x[0] <= 0) flag = F_AMPLITUDE;
@@ -758,11 +805,12 @@ int state_stride(int method)
     return m == 0 ? StateLayout<5>::STRIDE : m == 1 ? StateLayout<4>::STRIDE : StateLayout<7>::STRIDE;
 }
 
-size_t scratch_bytes(int method, int n)
+size_t scratch_bytes(int method, int n, int precision)
 {
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t el = precision == 1 ? sizeof(double) : sizeof(float);
     return al(sizeof(int) * (size_t)n) * 2 + al(sizeof(int) * kMetaInts) +
-           al(sizeof(float) * (size_t)n * state_stride(method)) + al(sizeof(unsigned long long) * ST_N);
+           al(el * (size_t)n * state_stride(method)) + al(sizeof(unsigned long long) * ST_N);
 }
 
 void carve_scratch(void *base, int method, int n, Scratch *s)
@@ -777,7 +825,7 @@ void carve_scratch(void *base, int method, int n, Scratch *s)
     p += al(sizeof(int) * kMetaInts);
     s->stats = (unsigned long long *)p;
     p += al(sizeof(unsigned long long) * ST_N);
-    s->state = (float *)p;
+    s->state = (void *)p;
 }
 
 cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t stream, int *err_detail)
@@ -791,10 +839,18 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(s.stats, 0, sizeof(unsigned long long) * ST_N, stream);
     if (e != cudaSuccess) return e;
-    if (n == 0) return cudaSuccess;
+    if (n == 0) {
+        for (int k = 0; k < 4; ++k)
+            if (p.ev[k]) cudaEventRecord(p.ev[k], stream);
+        return cudaSuccess;
+    }
 
     const int r_cap = p.max_half_width > 0 ? (p.max_half_width < kMaxHalfWidth ? p.max_half_width : kMaxHalfWidth)
                                            : kMaxHalfWidth;
+    auto mark = [&](int k) {
+        if (p.ev[k]) cudaEventRecord(p.ev[k], stream);
+    };
+    mark(0);
     K0Args k0{(const Cand *)p.cands, n, p.n_frames, p.n_rows, p.n_cols, r_default, r_cap, p.method, ncol_total,
               p.out, p.flags, s.cls, s.meta};
     const int nb = (n + 255) / 256;
@@ -814,6 +870,7 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
         maxr = mr;
     }
     if (maxr > r_cap) maxr = r_cap;
+    mark(1);
     if (maxr >= 1) {
         const int side = 2 * maxr + 1;
         int tpb = p.threads_per_block > 0 ? p.threads_per_block : 128;
@@ -843,14 +900,25 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
         }
         if (e != cudaSuccess) return e;
     }
+    mark(2);
     K2Args k2{(const Cand *)p.cands, n, p.method, p.w0, r_default, s.state, state_stride(p.method), ncol_total,
-              p.out, p.flags, p.params_out};
-    switch (p.method) {
-    case 0: k2_finalize<0><<<nb, 256, 0, stream>>>(k2); break;
-    case 1: k2_finalize<1><<<nb, 256, 0, stream>>>(k2); break;
-    case 5: k2_finalize<5><<<nb, 256, 0, stream>>>(k2); break;
-    default: k2_finalize<7><<<nb, 256, 0, stream>>>(k2); break;
+              p.out, p.flags, p.params_out, p.diag};
+    if (p.precision == 1) {
+        switch (p.method) {
+        case 0: k2_finalize<0, double><<<nb, 256, 0, stream>>>(k2); break;
+        case 1: k2_finalize<1, double><<<nb, 256, 0, stream>>>(k2); break;
+        case 5: k2_finalize<5, double><<<nb, 256, 0, stream>>>(k2); break;
+        default: k2_finalize<7, double><<<nb, 256, 0, stream>>>(k2); break;
+        }
+    } else {
+        switch (p.method) {
+        case 0: k2_finalize<0, float><<<nb, 256, 0, stream>>>(k2); break;
+        case 1: k2_finalize<1, float><<<nb, 256, 0, stream>>>(k2); break;
+        case 5: k2_finalize<5, float><<<nb, 256, 0, stream>>>(k2); break;
+        default: k2_finalize<7, float><<<nb, 256, 0, stream>>>(k2); break;
+        }
     }
+    mark(3);
     return cudaGetLastError();
 }
 

@@ -14,7 +14,7 @@ struct Scratch {
     int *cls;            // n: ROI half-width class of each candidate, -1 if not enqueued
     int *order;          // n: enqueued candidates grouped by class
     int *meta;           // kMetaInts: class table (see loc_fit.cu)
-    float *state;        // n * state_stride(method): solver state for the finaliser
+    void *state;         // n * state_stride(method) elements of the solver precision
     unsigned long long *stats;  // 8 counters
 };
 
@@ -36,12 +36,14 @@ struct FitParams {
     int max_half_width;  // largest r present (known to the caller) or 0 = read back
     const float *init_params;
     float *params_out;
+    float *diag;
+    cudaEvent_t ev[4];   // optional: before the queue build, around the solver, after the finaliser
     double *out;
     uint8_t *flags;
 };
 
 int state_stride(int method);
-size_t scratch_bytes(int method, int n_cands);
+size_t scratch_bytes(int method, int n_cands, int precision);
 void carve_scratch(void *base, int method, int n_cands, Scratch *s);
 
 // Enqueue the whole fit on `stream`. Returns cudaSuccess or the launch error;

@@ -128,3 +128,30 @@ def make(w: Workload):
     rng = np.random.default_rng(w.seed)
     em = draw_emitters(w, rng)
     return render(w, em, rng), em
+
+
+def make_device(w: Workload, stream: int = 0):
+    """Frames rendered on the GPU (loc_synth_frames) for the workload's
+    emitters; returns (torch uint16-as-int16 tensor [f, y, x] on cuda,
+    Emitters). The emitter draw is the same as make()'s; the noise stream is
+    the device generator's, so frames differ from make()'s pixel by pixel."""
+    import torch
+
+    from . import lib
+    rng = np.random.default_rng(w.seed)
+    em = draw_emitters(w, rng)
+    bg = rng.uniform(*w.background, size=w.n_frames).astype(np.float32)
+    order = np.argsort(em.frame, kind="stable")
+    packed = np.stack([em.x[order], em.y[order], em.amplitude[order], em.sigma_x[order], em.sigma_y[order]],
+                      axis=1).astype(np.float32)
+    starts = np.searchsorted(em.frame[order], np.arange(w.n_frames + 1)).astype(np.int32)
+    d_em = torch.from_numpy(np.ascontiguousarray(packed)).cuda()
+    d_st = torch.from_numpy(starts).cuda()
+    d_bg = torch.from_numpy(bg).cuda()
+    frames = torch.empty((w.n_frames, w.size, w.size), dtype=torch.int16, device="cuda")
+    rc = lib().loc_synth_frames(frames.data_ptr(), w.n_frames, w.size, w.size, d_em.data_ptr(), d_st.data_ptr(),
+                                d_bg.data_ptr(), w.read_noise, w.seed, stream)
+    if rc != 0:
+        raise RuntimeError(f"loc_synth_frames failed: {rc}")
+    torch.cuda.synchronize()
+    return frames, em

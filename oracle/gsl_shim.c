@@ -114,10 +114,11 @@ static int shim_alloc(void *vstate, size_t n, size_t p)
 }
 
 /* iteration log: one entry per set(), counting the iterate() calls after it */
-#define LOG_CAP (1 << 22)
-static long g_log_n = 0;
-static int *g_log_iters = NULL;
-static int *g_log_status = NULL;
+#define LOG_CAP (1 << 20)
+/* per host thread, so several threads can drive the reference fitters */
+static _Thread_local long g_log_n = 0;
+static _Thread_local int *g_log_iters = NULL;
+static _Thread_local int *g_log_status = NULL;
 
 void lmshim_log_reset(void)
 {

@@ -3,6 +3,11 @@
 Gates (from the fitting path's definition): positions within 1e-3 px of the
 FP64 oracle and >= 99.9 % agreement of accept/reject flags. Other columns
 are compared with the tolerances written next to each check.
+
+Fits that reach the 200-iteration cap in the FP64 reference (termination
+status 1) have not converged: their final point depends on every rounding
+of a long wandering trajectory, so they count for flag agreement but not
+for the position gate; the tests assert that they are rare.
 """
 import numpy as np
 import pytest
@@ -28,10 +33,12 @@ def engine():
     e.close()
 
 
-def compare(rows, flags, ref_rows, ref_kept, method):
+def compare(rows, flags, ref_rows, ref_kept, method, ref_converged=None):
     kept = flags == 0
     agree = np.mean(kept == ref_kept) if len(kept) else 1.0
     both = kept & ref_kept
+    if ref_converged is not None:
+        both = both & ref_converged
     xi = XCOL[method]
     err = np.abs(rows[both, xi:xi + 2] - ref_rows[both, xi:xi + 2]).max(axis=1) if both.any() else np.zeros(0)
     frac = np.mean(err < POS_TOL) if len(err) else 1.0
@@ -43,7 +50,9 @@ def test_fp32_matches_reference_golden(engine, name, method):
     g = G.load(name)
     rows, flags = engine.fit_host(g["frames"], g["cands"], method, g["w0"])
     ref_kept = g[f"kept_{method}"] == 1
-    agree, frac, err, both = compare(rows, flags, g[f"out_{method}"], ref_kept, method)
+    capped = g[f"iters_{method}"] >= 200
+    assert np.mean(capped) < 0.03
+    agree, frac, err, both = compare(rows, flags, g[f"out_{method}"], ref_kept, method, ~capped)
     n = len(flags)
     # small fixtures: at most one disagreement where 0.1 % of n is below one
     assert np.sum((flags == 0) != ref_kept) <= max(1, int(0.001 * n)), (agree, np.nonzero((flags == 0) != ref_kept))
@@ -58,9 +67,10 @@ def test_fp64_gpu_path_matches_oracle(engine, name, method):
     opts = L.default_options(precision=1)
     rows, flags = engine.fit_host(g["frames"], g["cands"], method, g["w0"], options=opts)
     out, oflags, _, _ = O.fit(g["frames"], g["cands"], method, g["w0"])
-    agree, frac, err, both = compare(rows, flags, out, oflags == 0, method)
+    ncol = O.REF_COLUMNS[method]
+    agree, frac, err, both = compare(rows, flags, out, oflags == 0, method, out[:, ncol + 1] != 1)
     assert np.sum(flags != oflags) <= 1
-    assert np.mean(err < POS_TOL_FP64) >= 0.99
+    assert np.all(err < POS_TOL_FP64), np.sort(err)[-3:]
     ncol = O.REF_COLUMNS[method]
     # iteration counts follow the FP64 oracle step for step
     assert np.mean(rows[:, ncol] == out[:, ncol]) >= 0.98
@@ -81,20 +91,21 @@ def test_fp32_matches_oracle_seeded(engine, wname, method, n_frames):
     w, frames, cands = _workload(wname, n_frames)
     rows, flags = engine.fit_host(frames, cands, method, w.w0)
     out, oflags, _, _ = O.fit(frames, cands, method, w.w0, nthreads=8)
-    agree, frac, err, both = compare(rows, flags, out, oflags == 0, method)
+    ncol = O.REF_COLUMNS[method]
+    capped = out[:, ncol + 1] == 1
+    assert np.mean(capped) < 0.02
+    agree, frac, err, both = compare(rows, flags, out, oflags == 0, method, ~capped)
     assert agree >= FLAG_AGREEMENT or np.sum((flags == 0) != (oflags == 0)) <= 1, agree
     assert frac >= POS_FRACTION or np.sum(err >= POS_TOL) <= 1, (frac, np.sort(err)[-5:])
-    ncol = O.REF_COLUMNS[method]
     # widths / background / integral: relative 1e-3; uncertainties: 1e-2
     value_cols = {0: [1, 2, 5], 1: [1, 4], 5: [1, 2, 3, 7], 7: [1, 2, 3, 7]}[method]
     dev_cols = {0: [6, 7, 8, 9, 10], 1: [5, 6, 7, 8], 5: [11, 12, 14], 7: [11, 12, 14]}[method]
-    ok = both & (err < POS_TOL) if len(err) else both
     sel = np.nonzero(both)[0][err < POS_TOL]
     for cols, tol in ((value_cols, 1e-3), (dev_cols, 1e-2)):
         a, b = rows[sel][:, cols], out[sel][:, cols]
         rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-12)
         assert np.mean(rel.max(axis=1) < tol) >= 0.995, (cols, np.sort(rel.max(axis=1))[-5:])
-    assert ok.sum() > 0.5 * len(cands)
+    assert len(sel) > 0.5 * len(cands)
 
 
 def test_device_pointer_api_matches_host_api(engine):
@@ -135,7 +146,9 @@ def test_edge_cases(engine):
     assert list(flags[2:6]) == [10, 10, 10, 10]  # NaN, frame out of range (x2), half-width above the cap
     assert rows[1, 0] == 0 and np.isnan(rows[1, 1])
     out, oflags, _, _ = O.fit(frames, c, 0, 1.3)
-    np.testing.assert_array_equal(flags, oflags)
+    # the oracle accepts half-widths up to 64; the CUDA path caps them at 16
+    same = np.arange(len(c)) != 5
+    np.testing.assert_array_equal(flags[same], oflags[same])
     k = flags == 0
     np.testing.assert_allclose(rows[k, 3:5], out[k, 3:5], atol=POS_TOL)
 
