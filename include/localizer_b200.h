@@ -94,7 +94,9 @@ typedef struct loc_options {
     double epsrel;             /* test_delta relative tolerance; 1e-4 */
     int32_t precision;         /* LOC_PRECISION_* */
     float pivot_threshold;     /* FP32 Cholesky pivots below this fraction of
-                                  their diagonal are redone in FP64; 1e-4 */
+                                  their diagonal are redone in FP64 inside the
+                                  FP32 solver; 0 (default): off, ill-conditioned
+                                  fits are re-run in FP64 instead (fp64_rerun) */
     int32_t threads_per_block; /* 0: tuned default */
     int32_t blocks_per_sm;     /* 0: occupancy maximum */
     int32_t stage_u16;         /* -1: tuned; 0: ROI staged as float; 1: as uint16 */
@@ -116,6 +118,23 @@ typedef struct loc_options {
                                   of a solver branch decision, 1 if the fit was
                                   re-run in FP64, iterations and status of the
                                   FP32 run, reserved */
+    int32_t threads_per_fit;   /* threads cooperating on one fit in the first
+                                  scheduling level: 1 (default), 4 or 8 */
+    int32_t tail_threads_per_fit; /* threads per fit for fits that outlive the
+                                  first level's budget: 8 (default), 4 or 1 */
+    int32_t level0_budget;     /* solver iterations a fit may use in the first
+                                  level before it is suspended and finished by
+                                  the second; 0 = default (16), < 0 = one
+                                  level only */
+    int32_t fp64_rerun;        /* 0 (default): FP32 fits whose result could
+                                  depend on FP32 rounding are re-run entirely in
+                                  FP64 on the GPU (a solver branch decision within
+                                  rerun_margin of its threshold, an undamped pivot
+                                  ratio below rerun_pivot, or a stop for lack of
+                                  progress; fits that reach max_iter are not);
+                                  -1: never */
+    float rerun_margin;        /* 0: default 5e-4 */
+    float rerun_pivot;         /* 0: default 1e-3 */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */
@@ -188,6 +207,12 @@ typedef struct loc_stats {
     uint64_t iterations;
     uint64_t pixels_f;     /* sum over trial evaluations of ROI pixels */
     uint64_t pixels_j;     /* sum over Jacobian evaluations of ROI pixels */
+    uint64_t kcycles_refill;  /* thousands of SM cycles, summed over warps, spent */
+    uint64_t kcycles_step;    /* refilling fits, solving the damped step, in the */
+    uint64_t kcycles_pass;    /* pixel pass and in the accept/reject decision */
+    uint64_t kcycles_decide;
+    uint64_t fits_fp64_rerun;       /* fits re-run in FP64 after the FP32 solve */
+    uint64_t iterations_fp64_rerun; /* their solver iterations */
     float queue_ms;        /* device time of the work-queue build (-1 if not timed) */
     float solver_ms;       /* device time of the persistent solver kernel */
     float finalize_ms;     /* device time of the FP64 finaliser */

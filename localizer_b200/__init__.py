@@ -47,12 +47,16 @@ class Options(C.Structure):
     _fields_ = [("max_iter", C.c_int32), ("epsabs", C.c_double), ("epsrel", C.c_double),
                 ("precision", C.c_int32), ("pivot_threshold", C.c_float), ("threads_per_block", C.c_int32),
                 ("blocks_per_sm", C.c_int32), ("stage_u16", C.c_int32), ("max_half_width", C.c_int32),
-                ("d_init_params", C.c_void_p), ("d_params_out", C.c_void_p), ("d_diag", C.c_void_p)]
+                ("d_init_params", C.c_void_p), ("d_params_out", C.c_void_p), ("d_diag", C.c_void_p),
+                ("threads_per_fit", C.c_int32), ("tail_threads_per_fit", C.c_int32), ("level0_budget", C.c_int32),
+                ("fp64_rerun", C.c_int32), ("rerun_margin", C.c_float), ("rerun_pivot", C.c_float)]
 
 
 class Stats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("f_evals", "jacobian_evals", "lambda_solves", "fp64_escalations",
-                                          "fits", "iterations", "pixels_f", "pixels_j")] + \
+                                          "fits", "iterations", "pixels_f", "pixels_j", "kcycles_refill",
+                                          "kcycles_step", "kcycles_pass", "kcycles_decide", "fits_fp64_rerun",
+                                          "iterations_fp64_rerun")] + \
                [(n, C.c_float) for n in ("queue_ms", "solver_ms", "finalize_ms")]
 
     def as_dict(self):

@@ -76,7 +76,7 @@ LOC_API void loc_default_options(loc_options *opt)
     opt->epsabs = 1e-4;    // Localization.cpp:154
     opt->epsrel = 1e-4;
     opt->precision = LOC_PRECISION_FP32;
-    opt->pivot_threshold = 1e-4f;
+    opt->pivot_threshold = 0.0f;
     opt->threads_per_block = 0;
     opt->blocks_per_sm = 0;
     opt->stage_u16 = -1;
@@ -166,11 +166,12 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     if (!(o.epsrel >= 0) || !(o.epsabs >= 0)) return fail(LOC_E_INVALID, "negative tolerance");
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
-    const size_t need = locb::scratch_bytes(method, n_cands, o.precision);
+    const int rerun = o.fp64_rerun >= 0 ? 1 : 0;
+    const size_t need = locb::scratch_bytes(method, n_cands, o.precision, rerun);
     e = ctx->scratch.ensure(need);
     if (e != cudaSuccess) return fail(LOC_E_NOMEM, std::string("scratch allocation: ") + cudaGetErrorString(e));
     locb::Scratch s;
-    locb::carve_scratch(ctx->scratch.p, method, n_cands, &s);
+    locb::carve_scratch(ctx->scratch.p, method, n_cands, o.precision, rerun, &s);
     locb::FitParams p{};
     p.frames = d_frames;
     p.n_frames = n_frames;
@@ -185,10 +186,19 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     p.epsabs = o.epsabs;
     p.epsrel = o.epsrel;
     p.precision = o.precision;
-    p.pivot_thr = o.pivot_threshold > 0 ? o.pivot_threshold : 1e-4f;
+    p.pivot_thr = o.pivot_threshold > 0 ? o.pivot_threshold : 0.0f;
     p.threads_per_block = o.threads_per_block;
     p.blocks_per_sm = o.blocks_per_sm;
     p.max_half_width = o.max_half_width;
+    p.threads_per_fit = o.threads_per_fit > 0 ? o.threads_per_fit : 1;
+    p.tail_threads_per_fit = o.tail_threads_per_fit > 0 ? o.tail_threads_per_fit : 8;
+    p.level0_budget = o.level0_budget == 0 ? 16 : (o.level0_budget < 0 ? 0 : o.level0_budget);
+    p.fp64_rerun = rerun;
+    p.rerun_margin = o.rerun_margin > 0 ? o.rerun_margin : 5e-4f;
+    p.rerun_pivot = o.rerun_pivot > 0 ? o.rerun_pivot : 1e-3f;
+    if (!(p.threads_per_fit == 1 || p.threads_per_fit == 4 || p.threads_per_fit == 8) ||
+        !(p.tail_threads_per_fit == 1 || p.tail_threads_per_fit == 4 || p.tail_threads_per_fit == 8))
+        return fail(LOC_E_INVALID, "threads per fit must be 1, 4 or 8");
     p.init_params = o.d_init_params;
     p.params_out = o.d_params_out;
     p.diag = o.d_diag;
@@ -223,7 +233,7 @@ LOC_API int loc_last_stats(loc_ctx *ctx, loc_stats *st)
         std::memset(st, 0, sizeof(*st));
         return LOC_OK;
     }
-    unsigned long long v[8];
+    unsigned long long v[24];
     cudaError_t e = cudaMemcpy(v, ctx->stats_dev, sizeof(v), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(e, "stats copy");
     st->f_evals = v[0];
@@ -234,6 +244,12 @@ LOC_API int loc_last_stats(loc_ctx *ctx, loc_stats *st)
     st->iterations = v[5];
     st->pixels_f = v[6];
     st->pixels_j = v[7];
+    st->kcycles_refill = v[8];
+    st->kcycles_step = v[9];
+    st->kcycles_pass = v[10];
+    st->kcycles_decide = v[11];
+    st->fits_fp64_rerun = v[12 + 4];
+    st->iterations_fp64_rerun = v[12 + 5];
     st->queue_ms = st->solver_ms = st->finalize_ms = -1.0f;
     if (ctx->events_recorded && cudaEventSynchronize(ctx->ev[3]) == cudaSuccess) {
         cudaEventElapsedTime(&st->queue_ms, ctx->ev[0], ctx->ev[1]);

@@ -67,9 +67,10 @@ enum : uint8_t {
 enum : int { T_CONVERGED = 0, T_MAX_ITER = 1, T_EBADFUNC = 9, T_ENOPROG = 27, T_ETOLF = 29,
              T_ETOLX = 30, T_ETOLG = 31, T_SINGULAR = 64 };
 
-// stats slots
+// stats slots; the last four accumulate SM clock cycles per warp (lane 0)
+// spent in each phase of the solver loop
 enum { ST_F = 0, ST_J = 1, ST_LAMBDA = 2, ST_ESC = 3, ST_FITS = 4, ST_ITERS = 5, ST_PIXF = 6,
-       ST_PIXJ = 7, ST_N = 8 };
+       ST_PIXJ = 7, ST_CYC_REFILL = 8, ST_CYC_STEP = 9, ST_CYC_PASS = 10, ST_CYC_DECIDE = 11, ST_N = 12 };
 
 constexpr double kDblEps = 2.2204460492503131e-16;   // GSL_DBL_EPSILON
 constexpr float kLog2e = 1.4426950408889634f;
@@ -93,6 +94,20 @@ template <> struct Expo<double> {
     __device__ __forceinline__ static double ex(double a) { return exp(a); }
 };
 
+// Division, reciprocal and square roots of the solver's control path. In
+// FP32 they use the hardware approximations (about 2 ulp), which shortens
+// the serial dependency chains of the step solve and the accept/reject logic
+// (the FP32 path's accuracy is set elsewhere: by the accumulated normal
+// equations); the FP64 path keeps correctly rounded operations.
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float frcp(float a) { return __fdividef(1.0f, a); }
+__device__ __forceinline__ double frcp(double a) { return 1.0 / a; }
+__device__ __forceinline__ float frsqrt(float a) { return rsqrtf(a); }
+__device__ __forceinline__ double frsqrt(double a) { return rsqrt(a); }
+__device__ __forceinline__ float fsqrt(float a) { return a > 0.0f ? a * rsqrtf(a) : sqrtf(a); }
+__device__ __forceinline__ double fsqrt(double a) { return sqrt(a); }
+
 template <typename T> __device__ __forceinline__ T tiny_pos();
 template <> __device__ __forceinline__ float tiny_pos<float>() { return FLT_MIN; }
 template <> __device__ __forceinline__ double tiny_pos<double>() { return DBL_MIN; }
@@ -100,8 +115,10 @@ template <> __device__ __forceinline__ double tiny_pos<double>() { return DBL_MI
 // ---------------------------------------------------------------------------
 // Model + Jacobian + normal-equation accumulation over one ROI.
 //
-// roi: this lane's pixels in shared memory, pixel k = i + j*S at roi[k*ld]
-// (i along x). Parameters are ROI-local (x0 measured from the ROI origin).
+// roi: the fit's pixels in shared memory, pixel k = i + j*S at roi[k*ld]
+// (i along x). With TPF threads per fit, sub-lane q visits the columns
+// i = q, q + TPF, ... of every row and the caller sums the partial results
+// over the group. Parameters are ROI-local (x0 measured from the ROI origin).
 // acc receives the packed upper triangle of J^T J without its last entry
 // (the offset column is identically 1, so that entry is the pixel count),
 // vv = J^T r and chi2 = |r|^2, with r = model - data (unit noise weight;
@@ -143,8 +160,8 @@ __device__ __forceinline__ T expm1_series(T y)
 }
 
 // S > 0: compile-time ROI side (rows fully unrolled); S == 0: runtime side s_rt.
-template <int S, typename T>
-__device__ __forceinline__ void pass_sym(const float *__restrict__ roi, int ld, int s_rt, const T (&th)[5],
+template <int S, int TPF, typename T>
+__device__ __forceinline__ void pass_sym(const float *__restrict__ roi, int ld, int s_rt, int q, const T (&th)[5],
                                          const T (&dth)[5], T (&acc)[14], T (&vv)[5], T &chi2, T &dchi, T &dqmax)
 {
     const int s = S > 0 ? S : s_rt;
@@ -201,16 +218,20 @@ __device__ __forceinline__ void pass_sym(const float *__restrict__ roi, int ld, 
         const float *row = roi + j * s * ld;
         if (S > 0) {
 #pragma unroll
-            for (int i = 0; i < (S > 0 ? S : 1); ++i) body(i, wy, wy2, krow, row);
+            for (int t = 0; t < (S > 0 ? (S + TPF - 1) / TPF : 1); ++t) {
+                const int i = q + TPF * t;
+                if (TPF == 1 || i < S) body(i, wy, wy2, krow, row);
+            }
         } else {
 #pragma unroll 1
-            for (int i = 0; i < s; ++i) body(i, wy, wy2, krow, row);
+            for (int i = q; i < s; i += TPF) body(i, wy, wy2, krow, row);
         }
     }
 }
 
-template <int S, typename T>
-__device__ __forceinline__ void pass_fixed(const float *__restrict__ roi, int ld, int s_rt, T w0, const T (&th)[4],
+template <int S, int TPF, typename T>
+__device__ __forceinline__ void pass_fixed(const float *__restrict__ roi, int ld, int s_rt, int q, T w0,
+                                           const T (&th)[4],
                                            const T (&dth)[4], T (&acc)[9], T (&vv)[4], T &chi2, T &dchi, T &dqmax)
 {
     const int s = S > 0 ? S : s_rt;
@@ -255,16 +276,19 @@ __device__ __forceinline__ void pass_fixed(const float *__restrict__ roi, int ld
         const float *row = roi + j * s * ld;
         if (S > 0) {
 #pragma unroll
-            for (int i = 0; i < (S > 0 ? S : 1); ++i) body(i, wy, wy2, krow, row);
+            for (int t = 0; t < (S > 0 ? (S + TPF - 1) / TPF : 1); ++t) {
+                const int i = q + TPF * t;
+                if (TPF == 1 || i < S) body(i, wy, wy2, krow, row);
+            }
         } else {
 #pragma unroll 1
-            for (int i = 0; i < s; ++i) body(i, wy, wy2, krow, row);
+            for (int i = q; i < s; i += TPF) body(i, wy, wy2, krow, row);
         }
     }
 }
 
-template <int S, typename T>
-__device__ __forceinline__ void pass_ell(const float *__restrict__ roi, int ld, int s_rt, const T (&th)[7],
+template <int S, int TPF, typename T>
+__device__ __forceinline__ void pass_ell(const float *__restrict__ roi, int ld, int s_rt, int q, const T (&th)[7],
                                          const T (&dth)[7], T (&acc)[27], T (&vv)[7], T &chi2, T &dchi, T &dqmax)
 {
     const int s = S > 0 ? S : s_rt;
@@ -350,10 +374,13 @@ __device__ __forceinline__ void pass_ell(const float *__restrict__ roi, int ld, 
         const float *row = roi + j * s * ld;
         if (S > 0) {
 #pragma unroll
-            for (int i = 0; i < (S > 0 ? S : 1); ++i) body(i, wy, wy2, wc, wrb, brow, crow, row);
+            for (int t = 0; t < (S > 0 ? (S + TPF - 1) / TPF : 1); ++t) {
+                const int i = q + TPF * t;
+                if (TPF == 1 || i < S) body(i, wy, wy2, wc, wrb, brow, crow, row);
+            }
         } else {
 #pragma unroll 1
-            for (int i = 0; i < s; ++i) body(i, wy, wy2, wc, wrb, brow, crow, row);
+            for (int i = q; i < s; i += TPF) body(i, wy, wy2, wc, wrb, brow, crow, row);
         }
     }
 }
@@ -386,9 +413,9 @@ __device__ __forceinline__ int chol_solve(const MS (&Ms)[tri(P)], MS par, const 
             minpiv = (MS)mp;
             return thr > T(0) ? 1 : 2;
         }
-        const T l = sqrt(d);
-        inv[j] = T(1) / l;
-        L[pkl(j, j)] = l;
+        const T il = frsqrt(d);
+        inv[j] = il;
+        L[pkl(j, j)] = d * il;
 #pragma unroll
         for (int i = j + 1; i < P; ++i) {
             T sacc = (T)Ms[pku(P, j, i)];
@@ -417,10 +444,10 @@ __device__ __forceinline__ int chol_solve(const MS (&Ms)[tri(P)], MS par, const 
     T n2 = T(0);
 #pragma unroll
     for (int i = 0; i < P; ++i) n2 += zz[i] * zz[i];
-    const T zn = sqrt(n2);
+    const T zn = fsqrt(n2);
     T q2 = T(0);
     if (zn > T(0)) {
-        const T izn = T(1) / zn;
+        const T izn = frcp(zn);
         T qv[P];
 #pragma unroll
         for (int i = 0; i < P; ++i) {
@@ -438,6 +465,26 @@ __device__ __forceinline__ int chol_solve(const MS (&Ms)[tri(P)], MS par, const 
     return 0;
 }
 
+// FP64 refactorisation of an FP32 system whose pivot fell below threshold.
+// Kept out of line: it is rare, and inlined its double-precision working set
+// would raise the register budget of the whole solver loop.
+template <int P>
+__device__ __noinline__ int chol_solve_fp64(const float *Ms, float par, const float *g, float *z, float *out)
+{
+    float msl[tri(P)], gl[P], zl[P];
+#pragma unroll
+    for (int k = 0; k < tri(P); ++k) msl[k] = Ms[k];
+#pragma unroll
+    for (int k = 0; k < P; ++k) gl[k] = g[k];
+    float zn, w2, mp;
+    const int rc = chol_solve<P, double, float>(msl, par, gl, 0.0, zl, zn, w2, mp);
+#pragma unroll
+    for (int k = 0; k < P; ++k) z[k] = zl[k];
+    out[0] = zn;
+    out[1] = w2;
+    return rc;
+}
+
 // One damped solve in working precision T with FP64 escalation for float.
 template <int P, typename T>
 __device__ __forceinline__ int damped_solve(const T (&Ms)[tri(P)], T par, const T (&g)[P], float thr,
@@ -446,8 +493,21 @@ __device__ __forceinline__ int damped_solve(const T (&Ms)[tri(P)], T par, const 
     int rc = chol_solve<P, T, T>(Ms, par, g, (T)thr, z, znorm, w2, minpiv);
     if (rc == 1) {
         ++n_esc;
-        T mp2;
-        rc = chol_solve<P, double, T>(Ms, par, g, 0.0, z, znorm, w2, mp2);
+        if constexpr (sizeof(T) == 4) {
+            float msl[tri(P)], gl[P], zl[P], o2[2];
+#pragma unroll
+            for (int k = 0; k < tri(P); ++k) msl[k] = Ms[k];
+#pragma unroll
+            for (int k = 0; k < P; ++k) gl[k] = g[k];
+            rc = chol_solve_fp64<P>(msl, par, gl, zl, o2);
+#pragma unroll
+            for (int k = 0; k < P; ++k) z[k] = zl[k];
+            znorm = o2[0];
+            w2 = o2[1];
+        } else {
+            T mp2;
+            rc = chol_solve<P, double, T>(Ms, par, g, 0.0, z, znorm, w2, mp2);
+        }
     }
     return rc;
 }
@@ -468,7 +528,7 @@ __device__ __forceinline__ void lmpar_scaled(const T (&Ms)[tri(P)], const T (&g)
                                              T (&z)[P], float thr, unsigned &n_lambda, unsigned &n_esc,
                                              bool &singular, T &newton_piv, T &margin)
 {
-    const T idelta = T(1) / delta;
+    const T idelta = frcp(delta);
     T dxnorm, w2, mp;
     singular = false;
     ++n_lambda;
@@ -486,17 +546,17 @@ __device__ __forceinline__ void lmpar_scaled(const T (&Ms)[tri(P)], const T (&g)
         par = T(0);
         return;
     }
-    T par_l = (!rank_def && w2 > T(0)) ? fp / (delta * w2) : T(0);
+    T par_l = (!rank_def && w2 > T(0)) ? fdiv(fp * idelta, w2) : T(0);
     T gn2 = T(0);
 #pragma unroll
     for (int i = 0; i < P; ++i) gn2 += g[i] * g[i];
-    const T gnorm = sqrt(gn2);
-    T par_u = gnorm / delta;
+    const T gnorm = fsqrt(gn2);
+    T par_u = gnorm * idelta;
     if (par_u == T(0)) par_u = tiny_pos<T>() / (delta < T(0.1) ? delta : T(0.1));
     T pr = par;
     if (pr > par_u) pr = par_u;
     else if (pr < par_l) pr = par_l;
-    if (pr == T(0)) pr = gnorm / dxnorm;
+    if (pr == T(0)) pr = fdiv(gnorm, dxnorm);
     int fails = 0;
 #pragma unroll 1
     for (int it = 1;; ++it) {
@@ -523,7 +583,7 @@ __device__ __forceinline__ void lmpar_scaled(const T (&Ms)[tri(P)], const T (&g)
         if (par_l == T(0) && fp_old < T(0)) margin = fmin(margin, fabs(fp - fp_old) * idelta);
         if (par_l == T(0) && fp <= fp_old && fp_old < T(0)) break;
         if (it == 10) break;
-        const T par_c = fp / (delta * w2);
+        const T par_c = fdiv(fp * idelta, w2);
         if (fp > T(0)) {
             if (pr > par_l) par_l = pr;
         } else if (fp < T(0)) {

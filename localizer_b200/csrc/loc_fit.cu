@@ -25,10 +25,12 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int K = kMaxHalfWidth + 1;
 constexpr int M_NCLS = 0, M_MAXR = 1;
-__host__ __device__ constexpr int m_side(int c) { return 8 + 0 * K + c; }
-__host__ __device__ constexpr int m_start(int c) { return 8 + 1 * K + c; }
-__host__ __device__ constexpr int m_count(int c) { return 8 + 2 * K + c; }
-__host__ __device__ constexpr int m_next(int c) { return 8 + 3 * K + c; }
+// per ROI half-width r: queue start, count, dequeue cursor, histogram, fill cursor
+__host__ __device__ constexpr int m_start(int r) { return 8 + 1 * K + r; }
+__host__ __device__ constexpr int m_count(int r) { return 8 + 2 * K + r; }
+__host__ __device__ constexpr int m_next(int r) { return 8 + 3 * K + r; }
+__host__ __device__ constexpr int m_ccount(int r) { return 8 + 6 * K + r; }
+__host__ __device__ constexpr int m_cnext(int r) { return 8 + 7 * K + r; }
 __host__ __device__ constexpr int m_hist(int r) { return 8 + 4 * K + r; }
 __host__ __device__ constexpr int m_fill(int r) { return 8 + 5 * K + r; }
 
@@ -90,7 +92,7 @@ __global__ void k0_classify(K0Args a)
         if (hist[r]) atomicAdd(&a.meta[m_hist(r)], hist[r]);
 }
 
-// One block: class table in descending half-width order.
+// One block: queue layout per half-width, largest ROIs first.
 __global__ void k0_classes(int *meta)
 {
     if (threadIdx.x != 0) return;
@@ -99,10 +101,9 @@ __global__ void k0_classes(int *meta)
         const int cnt = meta[m_hist(r)];
         if (cnt == 0) continue;
         if (r > maxr) maxr = r;
-        meta[m_side(ncls)] = 2 * r + 1;
-        meta[m_start(ncls)] = start;
-        meta[m_count(ncls)] = cnt;
-        meta[m_next(ncls)] = 0;
+        meta[m_start(r)] = start;
+        meta[m_count(r)] = cnt;
+        meta[m_next(r)] = 0;
         meta[m_fill(r)] = start;
         start += cnt;
         ++ncls;
@@ -127,6 +128,41 @@ __global__ void k0_scatter(const int *cls, int n, int *meta, int *order)
     order[base + __popc(peers & ((1u << lane) - 1))] = i;
 }
 
+// Fits of the FP32 solver whose result could depend on its rounding go to an
+// FP64 re-run: a branch decision of the trust-region method was within
+// `margin` of its threshold, the undamped normal matrix had a pivot ratio
+// below `pivot` (ill-conditioned), or the solver stopped for lack of
+// progress.
+template <int P>
+__global__ void k3_flag(const float *state32, int stride, const int *cls, const uint8_t *flags, int n, float margin,
+                        float pivot, int *cls2, int *meta2)
+{
+    using SL = StateLayout<P>;
+    __shared__ int hist[K];
+    for (int r = threadIdx.x; r < K; r += blockDim.x) hist[r] = 0;
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        int c2 = -1;
+        if (cls[i] >= 0 && flags[i] == F_PENDING) {
+            const float *s = state32 + (size_t)i * stride;
+            // fits stopped by the iteration cap are left alone: they have not
+            // converged, are almost always rejected, and cost 200 iterations
+            const float status = s[SL::STATUS];
+            const bool risky = status != (float)T_MAX_ITER &&
+                               (s[SL::MARGIN] < margin || s[SL::MINPIV] < pivot || status != 0.0f);
+            if (risky) {
+                c2 = cls[i];
+                atomicAdd(&hist[c2], 1);
+            }
+        }
+        cls2[i] = c2;
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < K; r += blockDim.x)
+        if (hist[r]) atomicAdd(&meta2[m_hist(r)], hist[r]);
+}
+
 struct K1Args {
     const uint16_t *frames;
     long long frame_px;
@@ -144,51 +180,92 @@ struct K1Args {
     float pivot_thr;
     const float *init_params;
     unsigned long long *stats;
+    int level;          // 0: fresh candidates, 1: fits suspended by level 0
+    int budget;         // level-0 iteration budget (0: none)
+    int *cont;          // continuation queue, laid out like order
+    float *cont_state;  // saved solver state of suspended fits
+    int cont_stride;
 };
 
-template <int METHOD, int S, typename T> struct Pass;
-template <int S, typename T> struct Pass<0, S, T> {
-    __device__ __forceinline__ static void run(const float *roi, int ld, int s, T, const T (&te)[5], const T (&dt)[5],
+template <int METHOD, int S, int TPF, typename T> struct Pass;
+template <int S, int TPF, typename T> struct Pass<0, S, TPF, T> {
+    __device__ __forceinline__ static void run(const float *roi, int s, int q, T, const T (&te)[5], const T (&dt)[5],
                                                T (&acc)[14], T (&vv)[5], T &chi2, T &dchi, T &dqmax)
     {
-        pass_sym<S, T>(roi, ld, s, te, dt, acc, vv, chi2, dchi, dqmax);
+        pass_sym<S, TPF, T>(roi, 1, s, q, te, dt, acc, vv, chi2, dchi, dqmax);
     }
 };
-template <int S, typename T> struct Pass<1, S, T> {
-    __device__ __forceinline__ static void run(const float *roi, int ld, int s, T w0, const T (&te)[4],
+template <int S, int TPF, typename T> struct Pass<1, S, TPF, T> {
+    __device__ __forceinline__ static void run(const float *roi, int s, int q, T w0, const T (&te)[4],
                                                const T (&dt)[4], T (&acc)[9], T (&vv)[4], T &chi2, T &dchi,
                                                T &dqmax)
     {
-        pass_fixed<S, T>(roi, ld, s, w0, te, dt, acc, vv, chi2, dchi, dqmax);
+        pass_fixed<S, TPF, T>(roi, 1, s, q, w0, te, dt, acc, vv, chi2, dchi, dqmax);
     }
 };
-template <int S, typename T> struct Pass<7, S, T> {
-    __device__ __forceinline__ static void run(const float *roi, int ld, int s, T, const T (&te)[7], const T (&dt)[7],
+template <int S, int TPF, typename T> struct Pass<7, S, TPF, T> {
+    __device__ __forceinline__ static void run(const float *roi, int s, int q, T, const T (&te)[7], const T (&dt)[7],
                                                T (&acc)[27], T (&vv)[7], T &chi2, T &dchi, T &dqmax)
     {
-        pass_ell<S, T>(roi, ld, s, te, dt, acc, vv, chi2, dchi, dqmax);
+        pass_ell<S, TPF, T>(roi, 1, s, q, te, dt, acc, vv, chi2, dchi, dqmax);
     }
 };
 
-// Process one ROI class with the whole warp; S > 0 compile-time side.
-template <int METHOD, typename T, int S>
-__device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsigned (&st)[ST_N])
+// Shared-memory words per fit for a ROI of npx pixels and TPF threads per
+// fit: the smallest stride >= npx with stride = TPF (mod 2 TPF), so that the
+// 32 lanes of a warp (32/TPF fits, TPF columns each) hit 32 distinct banks.
+__host__ __device__ constexpr int roi_stride(int npx, int tpf)
+{
+    return npx + ((tpf - npx % (2 * tpf)) + 2 * tpf) % (2 * tpf);
+}
+
+template <typename T>
+__device__ __forceinline__ T group_sum(T v, int tpf, unsigned mask)
+{
+    for (int o = tpf >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T group_max(T v, int tpf, unsigned mask)
+{
+    for (int o = tpf >> 1; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(mask, v, o));
+    return v;
+}
+
+// Saved solver state of a suspended fit (continuation level), floats:
+// parameters, J^T J, J^T f, D, last step, then 11 scalars.
+template <int P> struct ContLayout {
+    static constexpr int NT = tri(P);
+    static constexpr int TH = 0, A = P, V = P + NT, D = 2 * P + NT, DX = 3 * P + NT, SC = 4 * P + NT;
+    static constexpr int STRIDE = ((SC + 11) + 3) / 4 * 4;
+};
+
+// Process one queue of ROI half-width r: the fresh candidates (level 0) or
+// the fits suspended there (level 1). TPF threads cooperate on each fit;
+// S = 2r + 1 at compile time, or 0 for a runtime side.
+template <int METHOD, typename T, int S, int TPF>
+__device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, unsigned (&st)[ST_N])
 {
     constexpr int P = Traits<METHOD>::P;
     constexpr int NT = tri(P);
     constexpr int IX = Traits<METHOD>::IX;
     using SL = StateLayout<P>;
-    const int ld = blockDim.x;
+    using CL = ContLayout<P>;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
-    const int wbase = tid - lane;
-    const int s = S > 0 ? S : a.meta[m_side(c)];
-    const int r = (s - 1) / 2;
+    const int q = lane % TPF;            // sub-lane within the fit's group
+    const int glead = lane - q;          // lane of the group leader
+    const bool leader = q == 0;
+    const int s = S > 0 ? S : 2 * r + 1;
     const int npx = s * s;
-    const int cstart = a.meta[m_start(c)];
-    const int ccount = a.meta[m_count(c)];
-    int *next = a.meta + m_next(c);
-    const float *myroi = smem + tid;
+    const int stride = roi_stride(npx, TPF);
+    const float *myroi = smem + (tid / TPF) * stride;
+    const bool cont = a.level == 1;
+    const int *queue = cont ? a.cont : a.order;
+    const int cstart = a.meta[m_start(r)];
+    const int ccount = a.meta[cont ? m_ccount(r) : m_count(r)];
+    int *next = a.meta + (cont ? m_cnext(r) : m_next(r));
     const T inv_s2 = sizeof(T) == 4 ? (T)a.inv_s2 : (T)a.inv_s2_d;
     const T inv_abs_s = sizeof(T) == 4 ? (T)a.inv_abs_s : (T)a.inv_abs_s_d;
     const T w0 = (T)a.w0;
@@ -209,29 +286,61 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
         return k == IX ? t[k] + (T)xo : (k == IX + 1 ? t[k] + (T)yo : t[k]);
     };
     auto finish = [&](int status) {
-        T *o = (T *)a.state + (size_t)cidx * a.state_stride;
+        if (leader) {
+            T *o = (T *)a.state + (size_t)cidx * a.state_stride;
 #pragma unroll
-        for (int k = 0; k < P; ++k) o[k] = th[k];
+            for (int k = 0; k < P; ++k) o[k] = th[k];
 #pragma unroll
-        for (int k = 0; k < NT; ++k) o[P + k] = A[k];
-        o[SL::FNORM] = fnorm;
-        o[SL::ITERS] = (T)iterations;
-        o[SL::STATUS] = (T)status;
-        o[SL::XOFF] = (T)xo;
-        o[SL::YOFF] = (T)yo;
-        T lastr = T(0);
+            for (int k = 0; k < NT; ++k) o[P + k] = A[k];
+            o[SL::FNORM] = fnorm;
+            o[SL::ITERS] = (T)iterations;
+            o[SL::STATUS] = (T)status;
+            o[SL::XOFF] = (T)xo;
+            o[SL::YOFF] = (T)yo;
+            T lastr = T(0);
 #pragma unroll
-        for (int k = 0; k < P; ++k) {
-            const T tol = (T)a.epsabs + (T)a.epsrel * fabs(theta_abs(k, th));
-            const T q = fabs(dx[k]) / tol;
-            lastr = q > lastr ? q : lastr;
+            for (int k = 0; k < P; ++k) {
+                const T tol = (T)a.epsabs + (T)a.epsrel * fabs(theta_abs(k, th));
+                const T qq = fdiv(fabs(dx[k]), tol);
+                lastr = qq > lastr ? qq : lastr;
+            }
+            o[SL::MINPIV] = minpiv_fit;
+            o[SL::LASTR] = lastr;
+            o[SL::NESC] = (T)esc_fit;
+            o[SL::MARGIN] = margin_fit;
+            st[ST_FITS] += 1;
+            st[ST_ITERS] += iterations;
         }
-        o[SL::MINPIV] = minpiv_fit;
-        o[SL::LASTR] = lastr;
-        o[SL::NESC] = (T)esc_fit;
-        o[SL::MARGIN] = margin_fit;
-        st[ST_FITS] += 1;
-        st[ST_ITERS] += iterations;
+        phase = 0;
+    };
+    // park a fit that used up the first level's iteration budget
+    auto suspend = [&]() {
+        if (leader) {
+            float *o = a.cont_state + (size_t)cidx * a.cont_stride;
+#pragma unroll
+            for (int k = 0; k < P; ++k) {
+                o[CL::TH + k] = (float)th[k];
+                o[CL::V + k] = (float)v[k];
+                o[CL::D + k] = (float)D[k];
+                o[CL::DX + k] = (float)dx[k];
+            }
+#pragma unroll
+            for (int k = 0; k < NT; ++k) o[CL::A + k] = (float)A[k];
+            float *sc = o + CL::SC;
+            sc[0] = (float)fnorm;
+            sc[1] = (float)delta;
+            sc[2] = (float)par;
+            sc[3] = (float)xnorm;
+            sc[4] = __int_as_float(it_state);
+            sc[5] = __int_as_float(iterations);
+            sc[6] = (float)minpiv_fit;
+            sc[7] = (float)margin_fit;
+            sc[8] = __uint_as_float(esc_fit);
+            sc[9] = __int_as_float(xo);
+            sc[10] = __int_as_float(yo);
+            const int slot = atomicAdd(a.meta + m_ccount(r), 1);
+            a.cont[cstart + slot] = cidx;
+        }
         phase = 0;
     };
     auto test_delta = [&]() -> bool {
@@ -241,13 +350,17 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
         for (int k = 0; k < P; ++k) {
             const T tol = (T)a.epsabs + (T)a.epsrel * fabs(theta_abs(k, th));
             ok = ok && (fabs(dx[k]) < tol);
-            const T q = fabs(dx[k]) / tol;
-            worst = q > worst ? q : worst;
+            const T qq = fdiv(fabs(dx[k]), tol);
+            worst = qq > worst ? qq : worst;
         }
         margin_fit = fmin(margin_fit, fabs(worst - T(1)));
         return ok;
     };
     auto start_iteration = [&]() {
+        if (!cont && a.budget > 0 && iterations >= a.budget) {
+            suspend();
+            return;
+        }
         ++iterations;
         if (fnorm == T(0)) {  // iterate() returns at once; dx is unchanged
             if (test_delta()) finish(T_CONVERGED);
@@ -261,53 +374,86 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
         phase = 2;
     };
 
+    unsigned long long c_refill = 0, c_step = 0, c_pass = 0, c_decide = 0;
+    long long t_mark = clock64();
+    auto lap = [&](unsigned long long &acc_c) {
+        const long long t = clock64();
+        acc_c += (unsigned long long)(t - t_mark);
+        t_mark = t;
+    };
     while (true) {
-        // ---- refill idle lanes from the class queue ----
+        // ---- refill idle groups from the queue: one atomic per warp ----
         const bool want = (phase == 0) && !exhausted;
-        const unsigned need = __ballot_sync(kFull, want);
+        const unsigned need = __ballot_sync(kFull, want && leader);
         if (need) {
-            const int leader = __ffs(need) - 1;
+            const int first = __ffs(need) - 1;
             int base = 0;
-            if (lane == leader) base = atomicAdd(next, __popc(need));
-            base = __shfl_sync(kFull, base, leader);
+            if (lane == first) base = atomicAdd(next, __popc(need));
+            base = __shfl_sync(kFull, base, first);
             int my = -1;
             if (want) {
-                const int q = base + __popc(need & ((1u << lane) - 1));
-                if (q < ccount) my = a.order[cstart + q];
+                const int qi = base + __popc(need & ((1u << glead) - 1));
+                if (qi < ccount) my = queue[cstart + qi];
                 else exhausted = true;
             }
             int fr = 0;
             if (my >= 0) {
                 const Cand cd = a.cands[my];
-                xo = (int)floor(cd.x - (double)r);
-                yo = (int)floor(cd.y - (double)r);
                 fr = cd.frame;
                 cidx = my;
-                minpiv_fit = T(1);
-                margin_fit = T(1e30);
-                esc_fit = 0;
-                if (a.init_params) {
-                    const float *ip = a.init_params + (size_t)my * P;
+                if (cont) {
+                    const float *o = a.cont_state + (size_t)my * a.cont_stride;
 #pragma unroll
                     for (int k = 0; k < P; ++k) {
-                        const double off = k == IX ? (double)xo : (k == IX + 1 ? (double)yo : 0.0);
-                        th[k] = (T)((double)ip[k] - off);
+                        th[k] = (T)o[CL::TH + k];
+                        v[k] = (T)o[CL::V + k];
+                        D[k] = (T)o[CL::D + k];
+                        dx[k] = (T)o[CL::DX + k];
                     }
+#pragma unroll
+                    for (int k = 0; k < NT; ++k) A[k] = (T)o[CL::A + k];
+                    const float *sc = o + CL::SC;
+                    fnorm = (T)sc[0];
+                    delta = (T)sc[1];
+                    par = (T)sc[2];
+                    xnorm = (T)sc[3];
+                    it_state = __float_as_int(sc[4]);
+                    iterations = __float_as_int(sc[5]);
+                    minpiv_fit = (T)sc[6];
+                    margin_fit = (T)sc[7];
+                    esc_fit = __float_as_uint(sc[8]);
+                    xo = __float_as_int(sc[9]);
+                    yo = __float_as_int(sc[10]);
+                    phase = 3;  // resume: start the next outer iteration after staging
                 } else {
-                    const T xl = (T)(cd.x - (double)xo), yl = (T)(cd.y - (double)yo);
-                    if constexpr (METHOD == 0) {
-                        th[0] = (T)cd.intensity; th[1] = w0; th[2] = xl; th[3] = yl; th[4] = (T)cd.background;
-                    } else if constexpr (METHOD == 1) {
-                        th[0] = (T)cd.intensity; th[1] = xl; th[2] = yl; th[3] = (T)cd.background;
+                    xo = (int)floor(cd.x - (double)r);
+                    yo = (int)floor(cd.y - (double)r);
+                    minpiv_fit = T(1);
+                    margin_fit = T(1e30);
+                    esc_fit = 0;
+                    if (a.init_params) {
+                        const float *ip = a.init_params + (size_t)my * P;
+#pragma unroll
+                        for (int k = 0; k < P; ++k) {
+                            const double off = k == IX ? (double)xo : (k == IX + 1 ? (double)yo : 0.0);
+                            th[k] = (T)((double)ip[k] - off);
+                        }
                     } else {
-                        th[0] = (T)cd.intensity; th[1] = w0; th[2] = w0; th[3] = xl; th[4] = yl;
-                        th[5] = T(0); th[6] = (T)cd.background;
+                        const T xl = (T)(cd.x - (double)xo), yl = (T)(cd.y - (double)yo);
+                        if constexpr (METHOD == 0) {
+                            th[0] = (T)cd.intensity; th[1] = w0; th[2] = xl; th[3] = yl; th[4] = (T)cd.background;
+                        } else if constexpr (METHOD == 1) {
+                            th[0] = (T)cd.intensity; th[1] = xl; th[2] = yl; th[3] = (T)cd.background;
+                        } else {
+                            th[0] = (T)cd.intensity; th[1] = w0; th[2] = w0; th[3] = xl; th[4] = yl;
+                            th[5] = T(0); th[6] = (T)cd.background;
+                        }
                     }
+                    phase = 1;
                 }
-                phase = 1;
             }
             // warp-cooperative ROI staging: global uint16 -> shared float
-            unsigned got = __ballot_sync(kFull, my >= 0);
+            unsigned got = __ballot_sync(kFull, my >= 0 && leader);
             while (got) {
                 const int src = __ffs(got) - 1;
                 got &= got - 1;
@@ -315,17 +461,19 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
                 const int syo = __shfl_sync(kFull, yo, src);
                 const int sfr = __shfl_sync(kFull, fr, src);
                 const uint16_t *fb = a.frames + (size_t)sfr * (size_t)a.frame_px + sxo + (size_t)syo * a.n_rows;
-                float *dst = smem + wbase + src;
+                float *dst = smem + ((tid - lane + src) / TPF) * stride;
                 for (int k = lane; k < npx; k += 32) {
                     const int j = k / s, i = k - j * s;
-                    dst[k * ld] = (float)__ldg(fb + i + (size_t)j * a.n_rows);
+                    dst[k] = (float)__ldg(fb + i + (size_t)j * a.n_rows);
                 }
             }
             __syncwarp();
+            if (phase == 3) start_iteration();
         }
         if (__ballot_sync(kFull, phase != 0) == 0) break;
+        lap(c_refill);
 
-        // ---- choose this lane's evaluation point ----
+        // ---- choose this fit's evaluation point (identical in every sub-lane) ----
         bool do_pass = false;
         if (phase == 1) {
 #pragma unroll
@@ -336,7 +484,7 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
             T invD[P], g[P], Ms[NT], z[P];
 #pragma unroll
             for (int k = 0; k < P; ++k) {
-                invD[k] = T(1) / D[k];
+                invD[k] = frcp(D[k]);
                 g[k] = v[k] * invD[k];
             }
 #pragma unroll
@@ -347,8 +495,10 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
             bool sing = false;
             T npiv;
             lmpar_scaled<P, T>(Ms, g, delta, par, z, a.pivot_thr, nl, ne, sing, npiv, margin_fit);
-            st[ST_LAMBDA] += nl;
-            st[ST_ESC] += ne;
+            if (leader) {
+                st[ST_LAMBDA] += nl;
+                st[ST_ESC] += ne;
+            }
             esc_fit += ne;
             minpiv_fit = npiv < minpiv_fit ? npiv : minpiv_fit;
             if (sing) {
@@ -361,17 +511,17 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
                     te[k] = th[k] + dx[k];
                     pn2 += z[k] * z[k];
                 }
-                pnorm = sqrt(pn2);
+                pnorm = fsqrt(pn2);
                 if (it_state == 1 && pnorm < delta) delta = pnorm;
-                T q = T(0);
+                T qf = T(0);
 #pragma unroll
                 for (int i = 0; i < P; ++i) {
                     T row = T(0);
 #pragma unroll
                     for (int j = 0; j < P; ++j) row += Ms[i <= j ? pku(P, i, j) : pku(P, j, i)] * z[j];
-                    q += z[i] * row;
+                    qf += z[i] * row;
                 }
-                jdx2 = q;
+                jdx2 = qf;
                 const bool bad = (METHOD == 0 && te[1] == T(0)) || (METHOD == 7 && (te[1] == T(0) || te[2] == T(0)));
                 if (bad) finish(T_EBADFUNC);
                 else do_pass = true;
@@ -379,24 +529,42 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
         }
 
         // ---- the pass: model, Jacobian and normal equations at te ----
+        // All lanes reconverge here so that the pixel loop runs once for the
+        // whole warp rather than once per divergent group.
+        __syncwarp();
+        lap(c_step);
+        const unsigned pmask = __ballot_sync(kFull, do_pass);
         T acc[NT - 1], vv[P], chi2, dchi, dqmax;
         if (do_pass) {
             T dt[P];
 #pragma unroll
             for (int k = 0; k < P; ++k) dt[k] = phase == 2 ? dx[k] : T(0);
-            Pass<METHOD, S, T>::run(myroi, ld, s, w0, te, dt, acc, vv, chi2, dchi, dqmax);
-            if (phase == 1) {
-                st[ST_J] += 1;
-                st[ST_PIXJ] += npx;
-            } else {
-                st[ST_F] += 1;
-                st[ST_PIXF] += npx;
+            Pass<METHOD, S, TPF, T>::run(myroi, s, q, w0, te, dt, acc, vv, chi2, dchi, dqmax);
+            if constexpr (TPF > 1) {
+#pragma unroll
+                for (int k = 0; k < NT - 1; ++k) acc[k] = group_sum(acc[k], TPF, pmask);
+#pragma unroll
+                for (int k = 0; k < P; ++k) vv[k] = group_sum(vv[k], TPF, pmask);
+                chi2 = group_sum(chi2, TPF, pmask);
+                dchi = group_sum(dchi, TPF, pmask);
+                dqmax = group_max(dqmax, TPF, pmask);
+            }
+            if (leader) {
+                if (phase == 1) {
+                    st[ST_J] += 1;
+                    st[ST_PIXJ] += npx;
+                } else {
+                    st[ST_F] += 1;
+                    st[ST_PIXF] += npx;
+                }
             }
         }
 
+        __syncwarp();
+        lap(c_pass);
         // ---- decide ----
         if (do_pass) {
-            const T fn1 = sqrt(chi2) * inv_abs_s;
+            const T fn1 = fsqrt(chi2) * inv_abs_s;
             if (phase == 1) {
                 // gsl_multifit_fdfsolver_set for lmsder
 #pragma unroll
@@ -425,18 +593,18 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
                 if (T(0.1) * fn1 < fnorm) {
                     if (dqmax < T(0.25)) {
                         // accurate |f|^2 change from the per-pixel model differences
-                        actred = -(dchi * inv_s2) / (fnorm * fnorm);
+                        actred = fdiv(-(dchi * inv_s2), fnorm * fnorm);
                     } else {
-                        const T u = fn1 / fnorm;
+                        const T u = fdiv(fn1, fnorm);
                         actred = T(1) - u * u;
                     }
                 }
-                const T if2 = T(1) / (fnorm * fnorm);
+                const T if2 = frcp(fnorm * fnorm);
                 const T t1s = jdx2 * if2;
                 const T t2s = par * pnorm * pnorm * if2;
                 const T prered = t1s + T(2) * t2s;
                 const T dirder = -(t1s + t2s);
-                const T ratio = prered > T(0) ? actred / prered : T(0);
+                const T ratio = prered > T(0) ? fdiv(actred, prered) : T(0);
                 margin_fit = fmin(margin_fit, fmin(fabs(ratio - T(0.25)), fmin(fabs(ratio - T(0.75)),
                                                                               fabs(ratio - T(1e-4)))));
                 if (ratio > T(0.25)) {
@@ -445,7 +613,7 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
                         par *= T(0.5);
                     }
                 } else {
-                    T temp = (actred >= T(0)) ? T(0.5) : T(0.5) * dirder / (dirder + T(0.5) * actred);
+                    T temp = (actred >= T(0)) ? T(0.5) : fdiv(T(0.5) * dirder, dirder + T(0.5) * actred);
                     if (T(0.1) * fn1 >= fnorm || temp < T(0.1)) temp = T(0.1);
                     const T lim = pnorm / T(0.1);
                     delta = temp * (delta < lim ? delta : lim);
@@ -466,8 +634,10 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
                     xnorm = sqrt(xn2);
                     fnorm = fn1;
                     ++it_state;
-                    st[ST_J] += 1;  // the accepted trial's Jacobian
-                    st[ST_PIXJ] += npx;
+                    if (leader) {
+                        st[ST_J] += 1;  // the accepted trial's Jacobian
+                        st[ST_PIXJ] += npx;
+                    }
 #pragma unroll
                     for (int k = 0; k < P; ++k) {
                         const T cn = sqrt(A[pku(P, k, k)]);
@@ -481,10 +651,10 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
                     T gmax = T(0);
 #pragma unroll
                     for (int k = 0; k < P; ++k) {
-                        const T gk = fabs(v[k] / D[k]);
+                        const T gk = fabs(fdiv(v[k], D[k]));
                         if (gk > gmax) gmax = gk;
                     }
-                    const T gnorm = gmax / fnorm;
+                    const T gnorm = fdiv(gmax, fnorm);
                     if (fabs(actred) <= (T)kDblEps && prered <= (T)kDblEps && T(0.5) * ratio <= T(1))
                         finish(T_ETOLF);
                     else if (delta <= (T)kDblEps * xnorm)
@@ -496,35 +666,28 @@ __device__ __noinline__ void run_class(const K1Args &a, int c, float *smem, unsi
                 }
             }
         }
+        __syncwarp();
+        lap(c_decide);
+    }
+    if (lane == 0) {
+        st[ST_CYC_REFILL] += (unsigned)(c_refill >> 10);
+        st[ST_CYC_STEP] += (unsigned)(c_step >> 10);
+        st[ST_CYC_PASS] += (unsigned)(c_pass >> 10);
+        st[ST_CYC_DECIDE] += (unsigned)(c_decide >> 10);
     }
 }
 
-template <int METHOD, typename T>
-__global__ void __launch_bounds__(128) k1_lm_fit(K1Args a)
+// blocks of 128 threads resident per SM the register budget is sized for
+__host__ __device__ constexpr int k1_min_blocks(int method) { return method == 7 ? 2 : 3; }
+
+template <int METHOD, typename T, int S, int TPF>
+__global__ void __launch_bounds__(128, k1_min_blocks(METHOD)) k1_lm_fit(K1Args a, int r)
 {
     extern __shared__ float smem[];
     unsigned st[ST_N];
 #pragma unroll
     for (int k = 0; k < ST_N; ++k) st[k] = 0;
-    const int ncls = a.meta[M_NCLS];
-    for (int c = 0; c < ncls; ++c) {
-        const int s = a.meta[m_side(c)];
-        if constexpr (sizeof(T) == 8) {
-            run_class<METHOD, T, 0>(a, c, smem, st);
-            continue;
-        } else {
-        switch (s) {
-        case 5: run_class<METHOD, T, 5>(a, c, smem, st); break;
-        case 7: run_class<METHOD, T, 7>(a, c, smem, st); break;
-        case 9: run_class<METHOD, T, 9>(a, c, smem, st); break;
-        case 11: run_class<METHOD, T, 11>(a, c, smem, st); break;
-        case 13: run_class<METHOD, T, 13>(a, c, smem, st); break;
-        case 15: run_class<METHOD, T, 15>(a, c, smem, st); break;
-        case 17: run_class<METHOD, T, 17>(a, c, smem, st); break;
-        default: run_class<METHOD, T, 0>(a, c, smem, st); break;
-        }
-        }
-    }
+    if (a.meta[a.level == 1 ? m_ccount(r) : m_count(r)] > 0) run_class<METHOD, T, S, TPF>(a, r, smem, st);
     // warp-reduce the counters, one atomic per warp and counter
 #pragma unroll
     for (int k = 0; k < ST_N; ++k) {
@@ -541,7 +704,9 @@ struct K2Args {
     int method;
     double w0;
     int r_default;
-    const void *state;
+    const float *state32;   // FP32 solver state (NULL when the whole call ran in FP64)
+    const double *state64;  // FP64 solver state of re-run fits (or of every fit)
+    const int *rerun;       // >= 0 where the fit was re-run in FP64 (NULL: none)
     int state_stride;
     int ncol_total;
     double *out;
@@ -615,7 +780,7 @@ __device__ bool inverse_diagonal(const double (&A)[tri(P)], double (&cd)[P])
     return true;
 }
 
-template <int METHOD, typename ST>
+template <int METHOD>
 __global__ void k2_finalize(K2Args a)
 {
     constexpr int P = Traits<METHOD == 5 ? 7 : METHOD>::P;
@@ -625,10 +790,12 @@ __global__ void k2_finalize(K2Args a)
     if (i >= a.n) return;
     if (a.flags[i] != F_PENDING) return;
     const Cand cd = a.cands[i];
-    const ST *s = (const ST *)a.state + (size_t)i * a.state_stride;
-    const int iterations = (int)s[SL::ITERS];
-    const int status = (int)s[SL::STATUS];
-    const int xo = (int)s[SL::XOFF], yo = (int)s[SL::YOFF];
+    const bool r64 = a.state32 == nullptr || (a.rerun && a.rerun[i] >= 0);
+    const size_t base = (size_t)i * a.state_stride;
+    auto sv = [&](int k) -> double { return r64 ? a.state64[base + k] : (double)a.state32[base + k]; };
+    const int iterations = (int)sv(SL::ITERS);
+    const int status = (int)sv(SL::STATUS);
+    const int xo = (int)sv(SL::XOFF), yo = (int)sv(SL::YOFF);
     const int r = cd.half_width > 0 ? cd.half_width : a.r_default;
     const int xm = xo + 2 * r, ym = yo + 2 * r;
     const double w0 = a.w0;
@@ -641,7 +808,7 @@ __global__ void k2_finalize(K2Args a)
 
     double x[P];
 #pragma unroll
-    for (int k = 0; k < P; ++k) x[k] = (double)s[k];
+    for (int k = 0; k < P; ++k) x[k] = sv(k);
     constexpr int IX = METHOD == 0 ? 2 : METHOD == 1 ? 1 : 3;
     x[IX] += xo;
     x[IX + 1] += yo;
@@ -656,13 +823,14 @@ __global__ void k2_finalize(K2Args a)
     }
     if (a.diag) {
         float *dg = a.diag + (size_t)i * 8;
-        dg[0] = (float)s[SL::MINPIV];
-        dg[1] = (float)s[SL::LASTR];
-        dg[2] = (float)s[SL::NESC];
-        dg[3] = (float)s[SL::MARGIN];
-        dg[4] = 0.0f;
-        dg[5] = (float)iterations;
-        dg[6] = (float)status;
+        const size_t b32 = (size_t)i * a.state_stride;
+        dg[0] = (float)sv(SL::MINPIV);
+        dg[1] = (float)sv(SL::LASTR);
+        dg[2] = (float)sv(SL::NESC);
+        dg[3] = (float)sv(SL::MARGIN);
+        dg[4] = r64 && a.state32 != nullptr ? 1.0f : 0.0f;
+        dg[5] = a.state32 ? a.state32[b32 + SL::ITERS] : (float)iterations;
+        dg[6] = a.state32 ? a.state32[b32 + SL::STATUS] : (float)status;
         dg[7] = 0.0f;
     }
     uint8_t flag = F_KEPT;
@@ -674,8 +842,8 @@ __global__ void k2_finalize(K2Args a)
     }
     double A[NT];
 #pragma unroll
-    for (int k = 0; k < NT; ++k) A[k] = (double)s[P + k];
-    const double chi = (double)s[SL::FNORM];
+    for (int k = 0; k < NT; ++k) A[k] = sv(P + k);
+    const double chi = sv(SL::FNORM);
     double cv[P];
 
     if constexpr (METHOD == 0) {
@@ -780,10 +948,16 @@ __global__ void k2_finalize(K2Args a)
 
 int solver_method(int method) { return method == 5 ? 7 : method; }
 
-template <int METHOD, typename T>
-cudaError_t launch_k1(const K1Args &ka, int tpb, int bps_req, int smem, cudaStream_t stream)
+template <int METHOD, typename T, int S, int TPF>
+cudaError_t launch_k1_s(const K1Args &ka, int r, int tpb, int bps_req, cudaStream_t stream)
 {
-    auto kern = k1_lm_fit<METHOD, T>;
+    auto kern = k1_lm_fit<METHOD, T, S, TPF>;
+    const int side = 2 * r + 1;
+    const int per_fit = roi_stride(side * side, TPF) * (int)sizeof(float);
+    // fewer threads per block when the block's ROIs would not fit 227 KB
+    while (tpb > 32 && (tpb / TPF) * per_fit > 227 * 1024) tpb -= 32;
+    const int smem = (tpb / TPF) * per_fit;
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     int dev = 0, nsm = 0, bps = 0;
@@ -793,9 +967,47 @@ cudaError_t launch_k1(const K1Args &ka, int tpb, int bps_req, int smem, cudaStre
     if (e != cudaSuccess) return e;
     if (bps < 1) return cudaErrorInvalidConfiguration;
     if (bps_req > 0 && bps_req < bps) bps = bps_req;
-    kern<<<nsm * bps, tpb, smem, stream>>>(ka);
+    kern<<<nsm * bps, tpb, smem, stream>>>(ka, r);
     return cudaGetLastError();
 }
+
+template <int METHOD, typename T, int TPF>
+cudaError_t launch_k1_tpf(const K1Args &ka, int r, int tpb, int bps_req, cudaStream_t stream)
+{
+    if constexpr (sizeof(T) == 8) {
+        return launch_k1_s<METHOD, T, 0, TPF>(ka, r, tpb, bps_req, stream);
+    } else {
+        switch (2 * r + 1) {
+        case 5: return launch_k1_s<METHOD, T, 5, TPF>(ka, r, tpb, bps_req, stream);
+        case 7: return launch_k1_s<METHOD, T, 7, TPF>(ka, r, tpb, bps_req, stream);
+        case 9: return launch_k1_s<METHOD, T, 9, TPF>(ka, r, tpb, bps_req, stream);
+        case 11: return launch_k1_s<METHOD, T, 11, TPF>(ka, r, tpb, bps_req, stream);
+        case 13: return launch_k1_s<METHOD, T, 13, TPF>(ka, r, tpb, bps_req, stream);
+        case 15: return launch_k1_s<METHOD, T, 15, TPF>(ka, r, tpb, bps_req, stream);
+        case 17: return launch_k1_s<METHOD, T, 17, TPF>(ka, r, tpb, bps_req, stream);
+        default: return launch_k1_s<METHOD, T, 0, TPF>(ka, r, tpb, bps_req, stream);
+        }
+    }
+}
+
+// One persistent solver launch for the queue of half-width r with tpf
+// threads per fit (1, 4 or 8 for FP32; 1 or 8 for FP64).
+template <int METHOD, typename T>
+cudaError_t launch_k1(const K1Args &ka, int r, int tpb, int bps_req, int tpf, cudaStream_t stream)
+{
+    if constexpr (sizeof(T) == 8) {
+        return tpf == 8 ? launch_k1_tpf<METHOD, T, 8>(ka, r, tpb, bps_req, stream)
+                        : launch_k1_tpf<METHOD, T, 1>(ka, r, tpb, bps_req, stream);
+    } else {
+        switch (tpf) {
+        case 4: return launch_k1_tpf<METHOD, T, 4>(ka, r, tpb, bps_req, stream);
+        case 8: return launch_k1_tpf<METHOD, T, 8>(ka, r, tpb, bps_req, stream);
+        default: return launch_k1_tpf<METHOD, T, 1>(ka, r, tpb, bps_req, stream);
+        }
+    }
+}
+
+int cont_stride_of(int m) { return m == 0 ? ContLayout<5>::STRIDE : m == 1 ? ContLayout<4>::STRIDE : ContLayout<7>::STRIDE; }
 
 }  // namespace
 
@@ -805,28 +1017,84 @@ int state_stride(int method)
     return m == 0 ? StateLayout<5>::STRIDE : m == 1 ? StateLayout<4>::STRIDE : StateLayout<7>::STRIDE;
 }
 
-size_t scratch_bytes(int method, int n, int precision)
-{
-    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
-    const size_t el = precision == 1 ? sizeof(double) : sizeof(float);
-    return al(sizeof(int) * (size_t)n) * 2 + al(sizeof(int) * kMetaInts) +
-           al(el * (size_t)n * state_stride(method)) + al(sizeof(unsigned long long) * ST_N);
+// Scratch layout (256-byte aligned pieces): cls, order, meta, stats, cont,
+// cont_state, state (FP32 state, or FP64 state when the call runs in FP64),
+// then for the FP64 re-run of flagged fits: cls2, order2, meta2, state64.
+namespace {
+size_t al256(size_t b) { return (b + 255) / 256 * 256; }
 }
 
-void carve_scratch(void *base, int method, int n, Scratch *s)
+size_t scratch_bytes(int method, int n, int precision, int rerun)
 {
-    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t el = precision == 1 ? sizeof(double) : sizeof(float);
+    const int m = solver_method(method);
+    size_t b = al256(sizeof(int) * (size_t)n) * 2 + al256(sizeof(int) * kMetaInts) +
+               al256(sizeof(unsigned long long) * 2 * ST_N) + al256(sizeof(int) * (size_t)n) +
+               al256(sizeof(float) * (size_t)n * cont_stride_of(m)) + al256(el * (size_t)n * state_stride(method));
+    if (precision != 1 && rerun)
+        b += al256(sizeof(int) * (size_t)n) * 2 + al256(sizeof(int) * kMetaInts) +
+             al256(sizeof(double) * (size_t)n * state_stride(method));
+    return b;
+}
+
+void carve_scratch(void *base, int method, int n, int precision, int rerun, Scratch *s)
+{
+    const size_t el = precision == 1 ? sizeof(double) : sizeof(float);
     char *p = (char *)base;
     s->cls = (int *)p;
-    p += al(sizeof(int) * (size_t)n);
+    p += al256(sizeof(int) * (size_t)n);
     s->order = (int *)p;
-    p += al(sizeof(int) * (size_t)n);
+    p += al256(sizeof(int) * (size_t)n);
     s->meta = (int *)p;
-    p += al(sizeof(int) * kMetaInts);
+    p += al256(sizeof(int) * kMetaInts);
     s->stats = (unsigned long long *)p;
-    p += al(sizeof(unsigned long long) * ST_N);
+    p += al256(sizeof(unsigned long long) * 2 * ST_N);
+    s->cont = (int *)p;
+    p += al256(sizeof(int) * (size_t)n);
+    s->cont_state = (float *)p;
+    p += al256(sizeof(float) * (size_t)n * cont_stride_of(solver_method(method)));
     s->state = (void *)p;
+    p += al256(el * (size_t)n * state_stride(method));
+    if (precision != 1 && rerun) {
+        s->cls2 = (int *)p;
+        p += al256(sizeof(int) * (size_t)n);
+        s->order2 = (int *)p;
+        p += al256(sizeof(int) * (size_t)n);
+        s->meta2 = (int *)p;
+        p += al256(sizeof(int) * kMetaInts);
+        s->state64 = (double *)p;
+    } else {
+        s->cls2 = s->order2 = s->meta2 = nullptr;
+        s->state64 = nullptr;
+    }
 }
+
+namespace {
+
+template <typename T>
+cudaError_t launch_queues(const FitParams &p, const K1Args &k1_in, const int *counts, int r_cap, int tpb,
+                          bool two_level, int tpf_fixed, cudaStream_t stream, int *err_detail)
+{
+    K1Args k1 = k1_in;
+    const int m = solver_method(p.method);
+    cudaError_t e = cudaSuccess;
+    for (int level = 0; level < (two_level ? 2 : 1); ++level) {
+        k1.level = level;
+        k1.budget = two_level ? p.level0_budget : 0;
+        const int tpf = tpf_fixed > 0 ? tpf_fixed : (level == 0 ? p.threads_per_fit : p.tail_threads_per_fit);
+        for (int r = r_cap; r >= 1; --r) {
+            if (counts[r] <= 0) continue;
+            e = m == 0 ? launch_k1<0, T>(k1, r, tpb, p.blocks_per_sm, tpf, stream)
+              : m == 1 ? launch_k1<1, T>(k1, r, tpb, p.blocks_per_sm, tpf, stream)
+                       : launch_k1<7, T>(k1, r, tpb, p.blocks_per_sm, tpf, stream);
+            if (e == cudaErrorInvalidValue) *err_detail = 1;
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return e;
+}
+
+}  // namespace
 
 cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t stream, int *err_detail)
 {
@@ -834,10 +1102,12 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
     const int n = p.n_cands;
     const int ncol_total = ref_cols(p.method) + 2;
     const int r_default = (int)std::ceil(p.w0 * 4.0);
+    const bool rerun = p.precision != 1 && p.fp64_rerun && s.state64 != nullptr;
     cudaError_t e;
     e = cudaMemsetAsync(s.meta, 0, sizeof(int) * kMetaInts, stream);
     if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(s.stats, 0, sizeof(unsigned long long) * ST_N, stream);
+    if (rerun && (e = cudaMemsetAsync(s.meta2, 0, sizeof(int) * kMetaInts, stream)) != cudaSuccess) return e;
+    e = cudaMemsetAsync(s.stats, 0, sizeof(unsigned long long) * 2 * ST_N, stream);
     if (e != cudaSuccess) return e;
     if (n == 0) {
         for (int k = 0; k < 4; ++k)
@@ -859,64 +1129,69 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
     k0_scatter<<<nb, 256, 0, stream>>>(s.cls, n, s.meta, s.order);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
 
-    int maxr = p.max_half_width;
-    if (maxr <= 0) {
-        // the solver's shared memory is sized by the largest ROI present
-        int mr = 0;
-        e = cudaMemcpyAsync(&mr, s.meta + M_MAXR, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    // which half-width queues exist: known bound from the caller, or the
+    // histogram read back (one small synchronous copy)
+    int counts[K];
+    for (int r = 0; r < K; ++r) counts[r] = r <= r_cap ? 1 : 0;
+    if (p.max_half_width <= 0) {
+        e = cudaMemcpyAsync(counts, s.meta + m_count(0), sizeof(int) * K, cudaMemcpyDeviceToHost, stream);
         if (e != cudaSuccess) return e;
         e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return e;
-        maxr = mr;
     }
-    if (maxr > r_cap) maxr = r_cap;
     mark(1);
-    if (maxr >= 1) {
-        const int side = 2 * maxr + 1;
-        int tpb = p.threads_per_block > 0 ? p.threads_per_block : 128;
-        tpb = (tpb + 31) / 32 * 32;
-        if (tpb > 128) tpb = 128;
-        // shrink the block until the per-lane ROIs fit the 227 KB shared memory limit
-        while (tpb > 32 && (size_t)tpb * side * side * sizeof(float) > 227u * 1024u) tpb -= 32;
-        const size_t smem = (size_t)tpb * side * side * sizeof(float);
-        if (smem > 227u * 1024u) {
-            *err_detail = 1;
-            return cudaErrorInvalidValue;
-        }
-        const double s_abs = std::fabs(p.sigma);
-        K1Args k1{p.frames, (long long)p.n_rows * p.n_cols, p.n_rows, (const Cand *)p.cands, s.order, s.meta,
-                  s.state, state_stride(p.method), (float)p.w0, (float)(1.0 / (p.sigma * p.sigma)),
-                  (float)(1.0 / s_abs), 1.0 / (p.sigma * p.sigma), 1.0 / s_abs, p.max_iter, (float)p.epsabs,
-                  (float)p.epsrel, p.precision == 1 ? 0.0f : p.pivot_thr, p.init_params, s.stats};
-        const int m = solver_method(p.method);
-        if (p.precision == 1) {
-            e = m == 0 ? launch_k1<0, double>(k1, tpb, p.blocks_per_sm, (int)smem, stream)
-              : m == 1 ? launch_k1<1, double>(k1, tpb, p.blocks_per_sm, (int)smem, stream)
-                       : launch_k1<7, double>(k1, tpb, p.blocks_per_sm, (int)smem, stream);
-        } else {
-            e = m == 0 ? launch_k1<0, float>(k1, tpb, p.blocks_per_sm, (int)smem, stream)
-              : m == 1 ? launch_k1<1, float>(k1, tpb, p.blocks_per_sm, (int)smem, stream)
-                       : launch_k1<7, float>(k1, tpb, p.blocks_per_sm, (int)smem, stream);
-        }
-        if (e != cudaSuccess) return e;
-    }
-    mark(2);
-    K2Args k2{(const Cand *)p.cands, n, p.method, p.w0, r_default, s.state, state_stride(p.method), ncol_total,
-              p.out, p.flags, p.params_out, p.diag};
+    int tpb = p.threads_per_block > 0 ? p.threads_per_block : 128;
+    tpb = (tpb + 31) / 32 * 32;
+    if (tpb > 128) tpb = 128;
+    const double s_abs = std::fabs(p.sigma);
+    const int m = solver_method(p.method);
+    K1Args k1{p.frames, (long long)p.n_rows * p.n_cols, p.n_rows, (const Cand *)p.cands, s.order, s.meta,
+              s.state, state_stride(p.method), (float)p.w0, (float)(1.0 / (p.sigma * p.sigma)),
+              (float)(1.0 / s_abs), 1.0 / (p.sigma * p.sigma), 1.0 / s_abs, p.max_iter, (float)p.epsabs,
+              (float)p.epsrel, p.precision == 1 ? 0.0f : p.pivot_thr, p.init_params, s.stats,
+              0, 0, s.cont, s.cont_state, cont_stride_of(m)};
+    // level 0: every candidate, tpf0 threads per fit, up to `budget`
+    // iterations; level 1: the fits still running, tpf1 threads per fit
     if (p.precision == 1) {
-        switch (p.method) {
-        case 0: k2_finalize<0, double><<<nb, 256, 0, stream>>>(k2); break;
-        case 1: k2_finalize<1, double><<<nb, 256, 0, stream>>>(k2); break;
-        case 5: k2_finalize<5, double><<<nb, 256, 0, stream>>>(k2); break;
-        default: k2_finalize<7, double><<<nb, 256, 0, stream>>>(k2); break;
-        }
+        e = launch_queues<double>(p, k1, counts, r_cap, tpb, false, 1, stream, err_detail);
     } else {
-        switch (p.method) {
-        case 0: k2_finalize<0, float><<<nb, 256, 0, stream>>>(k2); break;
-        case 1: k2_finalize<1, float><<<nb, 256, 0, stream>>>(k2); break;
-        case 5: k2_finalize<5, float><<<nb, 256, 0, stream>>>(k2); break;
-        default: k2_finalize<7, float><<<nb, 256, 0, stream>>>(k2); break;
+        const bool two_level = p.level0_budget > 0 && p.level0_budget < p.max_iter;
+        e = launch_queues<float>(p, k1, counts, r_cap, tpb, two_level, 0, stream, err_detail);
+        if (e == cudaSuccess && rerun) {
+            // FP64 re-run of the fits whose FP32 result could depend on rounding
+            switch (m) {
+            case 0: k3_flag<5><<<nb, 256, 0, stream>>>((const float *)s.state, state_stride(p.method), s.cls, p.flags, n,
+                                                      p.rerun_margin, p.rerun_pivot, s.cls2, s.meta2); break;
+            case 1: k3_flag<4><<<nb, 256, 0, stream>>>((const float *)s.state, state_stride(p.method), s.cls, p.flags, n,
+                                                      p.rerun_margin, p.rerun_pivot, s.cls2, s.meta2); break;
+            default: k3_flag<7><<<nb, 256, 0, stream>>>((const float *)s.state, state_stride(p.method), s.cls, p.flags,
+                                                       n, p.rerun_margin, p.rerun_pivot, s.cls2, s.meta2); break;
+            }
+            k0_classes<<<1, 32, 0, stream>>>(s.meta2);
+            k0_scatter<<<nb, 256, 0, stream>>>(s.cls2, n, s.meta2, s.order2);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            K1Args k64 = k1;
+            k64.order = s.order2;
+            k64.meta = s.meta2;
+            k64.state = s.state64;
+            k64.pivot_thr = 0.0f;
+            k64.init_params = p.init_params;
+            k64.stats = s.stats + ST_N;  // counters of the re-run kept apart
+            // the flagged fits are the long, hard ones: several threads per fit
+            e = launch_queues<double>(p, k64, counts, r_cap, tpb, false, 8, stream, err_detail);
         }
+    }
+    if (e != cudaSuccess) return e;
+    mark(2);
+    K2Args k2{(const Cand *)p.cands, n, p.method, p.w0, r_default,
+              p.precision == 1 ? nullptr : (const float *)s.state,
+              p.precision == 1 ? (const double *)s.state : s.state64, rerun ? s.cls2 : nullptr,
+              state_stride(p.method), ncol_total, p.out, p.flags, p.params_out, p.diag};
+    switch (p.method) {
+    case 0: k2_finalize<0><<<nb, 256, 0, stream>>>(k2); break;
+    case 1: k2_finalize<1><<<nb, 256, 0, stream>>>(k2); break;
+    case 5: k2_finalize<5><<<nb, 256, 0, stream>>>(k2); break;
+    default: k2_finalize<7><<<nb, 256, 0, stream>>>(k2); break;
     }
     mark(3);
     return cudaGetLastError();

@@ -16,9 +16,15 @@ struct Scratch {
     int *meta;           // kMetaInts: class table (see loc_fit.cu)
     void *state;         // n * state_stride(method) elements of the solver precision
     unsigned long long *stats;  // 8 counters
+    int *cont;           // n: continuation queue (fits suspended after the level-0 budget)
+    float *cont_state;   // n * cont stride: their saved solver state
+    int *cls2;           // n: half-width class of fits re-run in FP64, -1 otherwise
+    int *order2;         // n: their queue
+    int *meta2;          // kMetaInts: its class table
+    double *state64;     // n * state_stride(method): FP64 state of re-run fits
 };
 
-constexpr int kMetaInts = 8 + 6 * (kMaxHalfWidth + 1);
+constexpr int kMetaInts = 8 + 8 * (kMaxHalfWidth + 1);
 
 struct FitParams {
     const uint16_t *frames;
@@ -34,6 +40,12 @@ struct FitParams {
     int threads_per_block;
     int blocks_per_sm;
     int max_half_width;  // largest r present (known to the caller) or 0 = read back
+    int threads_per_fit;       // level 0: 1, 4 or 8
+    int tail_threads_per_fit;  // level 1: 1, 4 or 8
+    int level0_budget;         // iterations before a fit moves to level 1 (0: single level)
+    int fp64_rerun;            // re-run flagged FP32 fits in FP64
+    float rerun_margin;        // branch-decision margin below which a fit is flagged
+    float rerun_pivot;         // undamped pivot ratio below which a fit is flagged
     const float *init_params;
     float *params_out;
     float *diag;
@@ -43,8 +55,8 @@ struct FitParams {
 };
 
 int state_stride(int method);
-size_t scratch_bytes(int method, int n_cands, int precision);
-void carve_scratch(void *base, int method, int n_cands, Scratch *s);
+size_t scratch_bytes(int method, int n_cands, int precision, int rerun);
+void carve_scratch(void *base, int method, int n_cands, int precision, int rerun, Scratch *s);
 
 // Enqueue the whole fit on `stream`. Returns cudaSuccess or the launch error;
 // *used_smem_side receives the ROI side the solver was sized for.

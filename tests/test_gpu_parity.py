@@ -105,7 +105,8 @@ def test_fp32_matches_oracle_seeded(engine, wname, method, n_frames):
         a, b = rows[sel][:, cols], out[sel][:, cols]
         rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-12)
         assert np.mean(rel.max(axis=1) < tol) >= 0.995, (cols, np.sort(rel.max(axis=1))[-5:])
-    assert len(sel) > 0.5 * len(cands)
+    # method 5 keeps only near-round spots (Localization.cpp:616-621)
+    assert len(sel) > (0.3 if method == 5 else 0.5) * len(cands)
 
 
 def test_device_pointer_api_matches_host_api(engine):
