@@ -124,7 +124,7 @@ typedef struct loc_options {
                                   first level's budget: 8 (default), 4 or 1 */
     int32_t level0_budget;     /* solver iterations a fit may use in the first
                                   level before it is suspended and finished by
-                                  the second; 0 = default (16), < 0 = one
+                                  the second; 0 = default (32), < 0 = one
                                   level only */
     int32_t fp64_rerun;        /* 0 (default): FP32 fits whose result could
                                   depend on FP32 rounding are re-run entirely in
@@ -133,8 +133,14 @@ typedef struct loc_options {
                                   ratio below rerun_pivot, or a stop for lack of
                                   progress; fits that reach max_iter are not);
                                   -1: never */
-    float rerun_margin;        /* 0: default 5e-4 */
-    float rerun_pivot;         /* 0: default 1e-3 */
+    float rerun_margin;        /* 0: default 1e-4 */
+    float rerun_pivot;         /* 0: default 1e-4 */
+    int32_t rerun_threads_per_fit; /* threads per fit of the FP64 re-run: 8
+                                  (default) or 1 */
+    int32_t serial_classes;    /* 0 (default): the ROI classes are solved as
+                                  concurrent chains on the context's auxiliary
+                                  streams, joined back to the call's stream;
+                                  1: all on the call's stream */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */
@@ -213,6 +219,8 @@ typedef struct loc_stats {
     uint64_t kcycles_decide;
     uint64_t fits_fp64_rerun;       /* fits re-run in FP64 after the FP32 solve */
     uint64_t iterations_fp64_rerun; /* their solver iterations */
+    uint64_t kcycles_fp64_rerun;    /* thousands of SM cycles (summed over warps) of the re-run */
+    uint64_t kcycles_fp64_rerun_pass; /* ... of which in the pixel pass */
     float queue_ms;        /* device time of the work-queue build (-1 if not timed) */
     float solver_ms;       /* device time of the persistent solver kernel */
     float finalize_ms;     /* device time of the FP64 finaliser */

@@ -49,14 +49,16 @@ class Options(C.Structure):
                 ("blocks_per_sm", C.c_int32), ("stage_u16", C.c_int32), ("max_half_width", C.c_int32),
                 ("d_init_params", C.c_void_p), ("d_params_out", C.c_void_p), ("d_diag", C.c_void_p),
                 ("threads_per_fit", C.c_int32), ("tail_threads_per_fit", C.c_int32), ("level0_budget", C.c_int32),
-                ("fp64_rerun", C.c_int32), ("rerun_margin", C.c_float), ("rerun_pivot", C.c_float)]
+                ("fp64_rerun", C.c_int32), ("rerun_margin", C.c_float), ("rerun_pivot", C.c_float),
+                ("rerun_threads_per_fit", C.c_int32), ("serial_classes", C.c_int32)]
 
 
 class Stats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("f_evals", "jacobian_evals", "lambda_solves", "fp64_escalations",
                                           "fits", "iterations", "pixels_f", "pixels_j", "kcycles_refill",
                                           "kcycles_step", "kcycles_pass", "kcycles_decide", "fits_fp64_rerun",
-                                          "iterations_fp64_rerun")] + \
+                                          "iterations_fp64_rerun", "kcycles_fp64_rerun",
+                                          "kcycles_fp64_rerun_pass")] + \
                [(n, C.c_float) for n in ("queue_ms", "solver_ms", "finalize_ms")]
 
     def as_dict(self):

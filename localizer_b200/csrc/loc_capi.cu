@@ -62,6 +62,9 @@ struct loc_ctx {
     unsigned long long *stats_dev = nullptr;  // points into scratch of the last call
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     bool events_recorded = false;
+    cudaStream_t aux[locb::kMaxAux] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[locb::kMaxAux] = {};
 };
 
 extern "C" {
@@ -119,6 +122,13 @@ LOC_API int loc_ctx_create(loc_ctx **ctx, int device)
             return cuda_fail(e, "cudaEventCreate");
         }
     }
+    if ((e = cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming)) != cudaSuccess)
+        return cuda_fail(e, "cudaEventCreate");
+    for (int k = 0; k < locb::kMaxAux; ++k) {
+        if ((e = cudaStreamCreateWithFlags(&c->aux[k], cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&c->join[k], cudaEventDisableTiming)) != cudaSuccess)
+            return cuda_fail(e, "auxiliary stream");
+    }
     *ctx = c;
     return LOC_OK;
 }
@@ -134,6 +144,11 @@ LOC_API int loc_ctx_destroy(loc_ctx *ctx)
     ctx->flags.release();
     for (int k = 0; k < 4; ++k)
         if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
+    if (ctx->fork) cudaEventDestroy(ctx->fork);
+    for (int k = 0; k < locb::kMaxAux; ++k) {
+        if (ctx->aux[k]) cudaStreamDestroy(ctx->aux[k]);
+        if (ctx->join[k]) cudaEventDestroy(ctx->join[k]);
+    }
     delete ctx;
     return LOC_OK;
 }
@@ -192,10 +207,11 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     p.max_half_width = o.max_half_width;
     p.threads_per_fit = o.threads_per_fit > 0 ? o.threads_per_fit : 1;
     p.tail_threads_per_fit = o.tail_threads_per_fit > 0 ? o.tail_threads_per_fit : 8;
-    p.level0_budget = o.level0_budget == 0 ? 16 : (o.level0_budget < 0 ? 0 : o.level0_budget);
+    p.level0_budget = o.level0_budget == 0 ? 32 : (o.level0_budget < 0 ? 0 : o.level0_budget);
     p.fp64_rerun = rerun;
-    p.rerun_margin = o.rerun_margin > 0 ? o.rerun_margin : 5e-4f;
-    p.rerun_pivot = o.rerun_pivot > 0 ? o.rerun_pivot : 1e-3f;
+    p.rerun_threads_per_fit = o.rerun_threads_per_fit == 1 ? 1 : 8;
+    p.rerun_margin = o.rerun_margin > 0 ? o.rerun_margin : 1e-4f;
+    p.rerun_pivot = o.rerun_pivot > 0 ? o.rerun_pivot : 1e-4f;
     if (!(p.threads_per_fit == 1 || p.threads_per_fit == 4 || p.threads_per_fit == 8) ||
         !(p.tail_threads_per_fit == 1 || p.tail_threads_per_fit == 4 || p.tail_threads_per_fit == 8))
         return fail(LOC_E_INVALID, "threads per fit must be 1, 4 or 8");
@@ -206,6 +222,11 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     cudaStreamIsCapturing((cudaStream_t)stream, &cap);
     for (int k = 0; k < 4; ++k) p.ev[k] = cap == cudaStreamCaptureStatusNone ? ctx->ev[k] : nullptr;
     ctx->events_recorded = cap == cudaStreamCaptureStatusNone;
+    for (int k = 0; k < locb::kMaxAux; ++k) {
+        p.aux[k] = o.serial_classes ? nullptr : ctx->aux[k];
+        p.join[k] = ctx->join[k];
+    }
+    p.fork = ctx->fork;
     p.out = d_out;
     p.flags = d_flags;
     int detail = 0;
@@ -250,6 +271,8 @@ LOC_API int loc_last_stats(loc_ctx *ctx, loc_stats *st)
     st->kcycles_decide = v[11];
     st->fits_fp64_rerun = v[12 + 4];
     st->iterations_fp64_rerun = v[12 + 5];
+    st->kcycles_fp64_rerun = v[12 + 8] + v[12 + 9] + v[12 + 10] + v[12 + 11];
+    st->kcycles_fp64_rerun_pass = v[12 + 10];
     st->queue_ms = st->solver_ms = st->finalize_ms = -1.0f;
     if (ctx->events_recorded && cudaEventSynchronize(ctx->ev[3]) == cudaSuccess) {
         cudaEventElapsedTime(&st->queue_ms, ctx->ev[0], ctx->ev[1]);

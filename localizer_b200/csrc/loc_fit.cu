@@ -48,6 +48,7 @@ struct K0Args {
     uint8_t *flags;
     int *cls;
     int *meta;
+    int *cls2;   // optional: FP64 re-run marks, cleared here
 };
 
 __device__ void write_reject_row(double *row, int ncol_total, int frame)
@@ -84,6 +85,7 @@ __global__ void k0_classify(K0Args a)
             }
         }
         a.cls[i] = cls;
+        if (a.cls2) a.cls2[i] = -1;
         a.flags[i] = flag;
         if (flag != F_PENDING) write_reject_row(a.out + (size_t)i * a.ncol_total, a.ncol_total, c.frame);
     }
@@ -161,6 +163,31 @@ __global__ void k3_flag(const float *state32, int stride, const int *cls, const 
     __syncthreads();
     for (int r = threadIdx.x; r < K; r += blockDim.x)
         if (hist[r]) atomicAdd(&meta2[m_hist(r)], hist[r]);
+}
+
+// Per-class form of the flag pass: walks the queue of half-width r and
+// appends the flagged fits to that class's FP64 queue (order2 / meta2).
+template <int P>
+__global__ void k3_flag_class(const float *state32, int stride, const int *order, const int *meta,
+                              const uint8_t *flags, int r, float margin, float pivot, int *cls2, int *order2,
+                              int *meta2)
+{
+    using SL = StateLayout<P>;
+    const int start = meta[m_start(r)], count = meta[m_count(r)];
+    if (blockIdx.x == 0 && threadIdx.x == 0) meta2[m_start(r)] = start;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+        const int i = order[start + t];
+        if (flags[i] != F_PENDING) continue;
+        const float *s = state32 + (size_t)i * stride;
+        const float status = s[SL::STATUS];
+        const bool risky = status != (float)T_MAX_ITER &&
+                           (s[SL::MARGIN] < margin || s[SL::MINPIV] < pivot || status != 0.0f);
+        if (risky) {
+            cls2[i] = r;
+            const int slot = atomicAdd(&meta2[m_count(r)], 1);
+            order2[start + slot] = i;
+        }
+    }
 }
 
 struct K1Args {
@@ -241,6 +268,26 @@ template <int P> struct ContLayout {
     static constexpr int STRIDE = ((SC + 11) + 3) / 4 * 4;
 };
 
+// Per-fit array that lives in registers, or (InSmem) in a shared-memory
+// slot of the fit's group; the FP64 solver keeps its normal equations there
+// so that they are not live in registers during the pixel pass.
+template <typename T, int N, bool InSmem> struct StateArr;
+template <typename T, int N> struct StateArr<T, N, false> {
+    T r[N];
+    __device__ __forceinline__ explicit StateArr(T *) {}
+    __device__ __forceinline__ T &operator[](int k) { return r[k]; }
+};
+template <typename T, int N> struct StateArr<T, N, true> {
+    T *p;
+    __device__ __forceinline__ explicit StateArr(T *slot) : p(slot) {}
+    __device__ __forceinline__ T &operator[](int k) { return p[k]; }
+};
+
+// Shared memory of the solver block: the ROIs, then (FP64 only) the
+// per-fit normal equations.
+template <typename T>
+__host__ __device__ constexpr int state_smem_per_fit(int P) { return sizeof(T) == 8 ? (tri(P) + P) * 8 : 0; }
+
 // Process one queue of ROI half-width r: the fresh candidates (level 0) or
 // the fits suspended there (level 1). TPF threads cooperate on each fit;
 // S = 2r + 1 at compile time, or 0 for a runtime side.
@@ -270,7 +317,15 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
     const T inv_abs_s = sizeof(T) == 4 ? (T)a.inv_abs_s : (T)a.inv_abs_s_d;
     const T w0 = (T)a.w0;
 
-    T th[P], A[NT], v[P], D[P], dx[P], te[P];
+    constexpr bool kSmemState = sizeof(T) == 8;
+    T *sstate = nullptr;
+    if constexpr (kSmemState) {
+        const int roi_bytes = (blockDim.x / TPF) * stride * (int)sizeof(float);
+        sstate = (T *)((char *)smem + ((roi_bytes + 15) / 16) * 16) + (tid / TPF) * (NT + P);
+    }
+    StateArr<T, NT, kSmemState> A(sstate);
+    StateArr<T, P, kSmemState> v(sstate + NT);
+    T th[P], D[P], dx[P], te[P];
     T fnorm = 0, delta = 0, par = 0, xnorm = 0, jdx2 = 0, pnorm = 0;
     int phase = 0, it_state = 0, iterations = 0, trial = 0, cidx = -1, xo = 0, yo = 0;
     T minpiv_fit = T(1);
@@ -678,10 +733,11 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
 }
 
 // blocks of 128 threads resident per SM the register budget is sized for
-__host__ __device__ constexpr int k1_min_blocks(int method) { return method == 7 ? 2 : 3; }
+// (FP64: one, i.e. the full 255 registers)
+__host__ __device__ constexpr int k1_min_blocks(int method, int bytes) { return bytes == 8 ? 1 : (method == 7 ? 2 : 3); }
 
 template <int METHOD, typename T, int S, int TPF>
-__global__ void __launch_bounds__(128, k1_min_blocks(METHOD)) k1_lm_fit(K1Args a, int r)
+__global__ void __launch_bounds__(128, k1_min_blocks(METHOD, sizeof(T))) k1_lm_fit(K1Args a, int r)
 {
     extern __shared__ float smem[];
     unsigned st[ST_N];
@@ -954,9 +1010,11 @@ cudaError_t launch_k1_s(const K1Args &ka, int r, int tpb, int bps_req, cudaStrea
     auto kern = k1_lm_fit<METHOD, T, S, TPF>;
     const int side = 2 * r + 1;
     const int per_fit = roi_stride(side * side, TPF) * (int)sizeof(float);
-    // fewer threads per block when the block's ROIs would not fit 227 KB
-    while (tpb > 32 && (tpb / TPF) * per_fit > 227 * 1024) tpb -= 32;
-    const int smem = (tpb / TPF) * per_fit;
+    constexpr int P = Traits<METHOD>::P;
+    auto smem_of = [&](int t) { return ((t / TPF) * per_fit + 15) / 16 * 16 + (t / TPF) * state_smem_per_fit<T>(P); };
+    // fewer threads per block when the block's shared memory would exceed 227 KB
+    while (tpb > 32 && smem_of(tpb) > 227 * 1024) tpb -= 32;
+    const int smem = smem_of(tpb);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
@@ -1122,7 +1180,7 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
     };
     mark(0);
     K0Args k0{(const Cand *)p.cands, n, p.n_frames, p.n_rows, p.n_cols, r_default, r_cap, p.method, ncol_total,
-              p.out, p.flags, s.cls, s.meta};
+              p.out, p.flags, s.cls, s.meta, rerun ? s.cls2 : nullptr};
     const int nb = (n + 255) / 256;
     k0_classify<<<nb, 256, 0, stream>>>(k0);
     k0_classes<<<1, 32, 0, stream>>>(s.meta);
@@ -1150,36 +1208,69 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
               (float)(1.0 / s_abs), 1.0 / (p.sigma * p.sigma), 1.0 / s_abs, p.max_iter, (float)p.epsabs,
               (float)p.epsrel, p.precision == 1 ? 0.0f : p.pivot_thr, p.init_params, s.stats,
               0, 0, s.cont, s.cont_state, cont_stride_of(m)};
-    // level 0: every candidate, tpf0 threads per fit, up to `budget`
-    // iterations; level 1: the fits still running, tpf1 threads per fit
-    if (p.precision == 1) {
-        e = launch_queues<double>(p, k1, counts, r_cap, tpb, false, 1, stream, err_detail);
-    } else {
-        const bool two_level = p.level0_budget > 0 && p.level0_budget < p.max_iter;
-        e = launch_queues<float>(p, k1, counts, r_cap, tpb, two_level, 0, stream, err_detail);
-        if (e == cudaSuccess && rerun) {
-            // FP64 re-run of the fits whose FP32 result could depend on rounding
-            switch (m) {
-            case 0: k3_flag<5><<<nb, 256, 0, stream>>>((const float *)s.state, state_stride(p.method), s.cls, p.flags, n,
-                                                      p.rerun_margin, p.rerun_pivot, s.cls2, s.meta2); break;
-            case 1: k3_flag<4><<<nb, 256, 0, stream>>>((const float *)s.state, state_stride(p.method), s.cls, p.flags, n,
-                                                      p.rerun_margin, p.rerun_pivot, s.cls2, s.meta2); break;
-            default: k3_flag<7><<<nb, 256, 0, stream>>>((const float *)s.state, state_stride(p.method), s.cls, p.flags,
-                                                       n, p.rerun_margin, p.rerun_pivot, s.cls2, s.meta2); break;
+    // Each ROI class is an independent chain -- level 0 (every candidate,
+    // tpf0 threads per fit, up to `budget` iterations), level 1 (the fits
+    // still running, tpf1 threads per fit), the flag pass and the FP64
+    // re-run of flagged fits -- forked onto the auxiliary streams so that the
+    // chains' tails overlap; the caller's stream joins them before the
+    // finaliser.
+    const bool two_level = p.precision != 1 && p.level0_budget > 0 && p.level0_budget < p.max_iter;
+    int naux = 0;
+    while (naux < kMaxAux && p.aux[naux]) ++naux;
+    if (naux > 0) {
+        e = cudaEventRecord(p.fork, stream);
+        if (e != cudaSuccess) return e;
+    }
+    bool used[kMaxAux] = {false};
+    int chain = 0;
+    for (int r = r_cap; r >= 1; --r) {
+        if (counts[r] <= 0) continue;
+        cudaStream_t cs = stream;
+        if (naux > 0) {
+            const int j = chain % naux;
+            cs = p.aux[j];
+            if (!used[j]) {
+                if ((e = cudaStreamWaitEvent(cs, p.fork, 0)) != cudaSuccess) return e;
+                used[j] = true;
             }
-            k0_classes<<<1, 32, 0, stream>>>(s.meta2);
-            k0_scatter<<<nb, 256, 0, stream>>>(s.cls2, n, s.meta2, s.order2);
-            if ((e = cudaGetLastError()) != cudaSuccess) return e;
-            K1Args k64 = k1;
-            k64.order = s.order2;
-            k64.meta = s.meta2;
-            k64.state = s.state64;
-            k64.pivot_thr = 0.0f;
-            k64.init_params = p.init_params;
-            k64.stats = s.stats + ST_N;  // counters of the re-run kept apart
-            // the flagged fits are the long, hard ones: several threads per fit
-            e = launch_queues<double>(p, k64, counts, r_cap, tpb, false, 8, stream, err_detail);
         }
+        ++chain;
+        int cnt1[K];
+        for (int q = 0; q < K; ++q) cnt1[q] = q == r ? 1 : 0;
+        if (p.precision == 1) {
+            e = launch_queues<double>(p, k1, cnt1, r_cap, tpb, false, 1, cs, err_detail);
+        } else {
+            e = launch_queues<float>(p, k1, cnt1, r_cap, tpb, two_level, 0, cs, err_detail);
+            if (e == cudaSuccess && rerun) {
+                const int fb = 2 * 148;
+                const float *st32 = (const float *)s.state;
+                const int sst = state_stride(p.method);
+                switch (m) {
+                case 0: k3_flag_class<5><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r, p.rerun_margin,
+                                                             p.rerun_pivot, s.cls2, s.order2, s.meta2); break;
+                case 1: k3_flag_class<4><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r, p.rerun_margin,
+                                                             p.rerun_pivot, s.cls2, s.order2, s.meta2); break;
+                default: k3_flag_class<7><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r,
+                                                              p.rerun_margin, p.rerun_pivot, s.cls2, s.order2,
+                                                              s.meta2); break;
+                }
+                if ((e = cudaGetLastError()) != cudaSuccess) return e;
+                K1Args k64 = k1;
+                k64.order = s.order2;
+                k64.meta = s.meta2;
+                k64.state = s.state64;
+                k64.pivot_thr = 0.0f;
+                k64.stats = s.stats + ST_N;  // counters of the re-run kept apart
+                // the flagged fits are the long, hard ones: several threads per fit
+                e = launch_queues<double>(p, k64, cnt1, r_cap, tpb, false, p.rerun_threads_per_fit, cs, err_detail);
+            }
+        }
+        if (e != cudaSuccess) return e;
+    }
+    for (int j = 0; j < naux; ++j) {
+        if (!used[j]) continue;
+        if ((e = cudaEventRecord(p.join[j], p.aux[j])) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(stream, p.join[j], 0)) != cudaSuccess) return e;
     }
     if (e != cudaSuccess) return e;
     mark(2);

@@ -7,6 +7,7 @@
 namespace locb {
 
 constexpr int kMaxHalfWidth = 16;  // LOC_MAX_HALF_WIDTH
+constexpr int kMaxAux = 4;         // auxiliary streams the per-class chains are spread over
 
 // Device scratch of one fit call. The caller provides the memory; sizes in
 // bytes come from scratch_bytes().
@@ -44,12 +45,16 @@ struct FitParams {
     int tail_threads_per_fit;  // level 1: 1, 4 or 8
     int level0_budget;         // iterations before a fit moves to level 1 (0: single level)
     int fp64_rerun;            // re-run flagged FP32 fits in FP64
+    int rerun_threads_per_fit; // 1 or 8
     float rerun_margin;        // branch-decision margin below which a fit is flagged
     float rerun_pivot;         // undamped pivot ratio below which a fit is flagged
     const float *init_params;
     float *params_out;
     float *diag;
     cudaEvent_t ev[4];   // optional: before the queue build, around the solver, after the finaliser
+    cudaStream_t aux[kMaxAux];  // optional auxiliary streams (NULL-terminated) for the class chains
+    cudaEvent_t fork;           // fork / join events for them
+    cudaEvent_t join[kMaxAux];
     double *out;
     uint8_t *flags;
 };
