@@ -79,6 +79,9 @@ _PROTOS = {
                                 C.c_double, C.c_double, C.POINTER(Options), C.c_void_p, C.c_void_p, C.c_void_p]),
     "loc_fit_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                C.c_double, C.c_double, C.POINTER(Options), C.c_void_p, C.c_void_p]),
+    "loc_fit_batch_static": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                       C.c_double, C.c_double, C.POINTER(Options), C.c_void_p, C.c_void_p,
+                                       C.c_void_p]),
     "loc_sync": (C.c_int, [C.c_void_p, C.c_void_p]),
     "loc_last_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "loc_compact_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int]),

@@ -15,10 +15,15 @@
 namespace {
 
 thread_local std::string g_err;
+// Messages recorded without heap allocation (by the allocation-free entry
+// point); the most recent of the two is what loc_last_error returns.
+thread_local char g_err_fixed[256];
+thread_local bool g_err_fixed_latest = false;
 
 int fail(int code, const std::string &msg)
 {
     g_err = msg;
+    g_err_fixed_latest = false;
     return code;
 }
 
@@ -69,7 +74,7 @@ struct loc_ctx {
 
 extern "C" {
 
-LOC_API const char *loc_last_error(void) { return g_err.c_str(); }
+LOC_API const char *loc_last_error(void) { return g_err_fixed_latest ? g_err_fixed : g_err.c_str(); }
 
 LOC_API void loc_default_options(loc_options *opt)
 {
@@ -336,6 +341,16 @@ LOC_API int loc_compact_host(const double *out, const uint8_t *flags, int n_cand
 }
 
 }  // extern "C"
+
+// Record an error message without allocating (used by loc_fit_batch_static).
+namespace locb {
+int record_error_fixed(int code, const char *msg)
+{
+    std::snprintf(g_err_fixed, sizeof(g_err_fixed), "%s", msg);
+    g_err_fixed_latest = true;
+    return code;
+}
+}  // namespace locb
 
 // ---- reference DLL compatibility (LocalizerDLL.h:53-56) ----
 
