@@ -108,7 +108,9 @@ typedef struct loc_options {
                                   larger candidates are flagged LOC_FLAG_BAD_INPUT */
     const float *d_init_params;/* optional device array, n_cands x p floats of
                                   absolute-coordinate start parameters (warm
-                                  start); NULL = reference start values */
+                                  start); NULL = reference start values; a NaN
+                                  first value selects the reference start for
+                                  that candidate */
     float *d_params_out;       /* optional device array, n_cands x p floats:
                                   raw fitted parameters (absolute coordinates) */
     float *d_diag;             /* optional device array, n_cands x 8 floats of
@@ -141,6 +143,17 @@ typedef struct loc_options {
                                   concurrent chains on the context's auxiliary
                                   streams, joined back to the call's stream;
                                   1: all on the call's stream */
+    const struct loc_proposal *proposal; /* optional trained start proposal
+                                  (loc_proposal_*) for this method: every
+                                  candidate's start is proposed by the network
+                                  and kept when its residual over the ROI is not
+                                  worse than the reference start's; NULL (default):
+                                  reference start values. Takes precedence over
+                                  d_init_params. */
+    int32_t warm_iter_limit;   /* with a proposal: warm-started fits that needed
+                                  more solver iterations than this are re-run
+                                  from the reference start (in FP64, the
+                                  reference's algorithm); 0: default 8, < 0: never */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */
@@ -245,6 +258,9 @@ typedef struct loc_stats {
     float queue_ms;        /* device time of the work-queue build (-1 if not timed) */
     float solver_ms;       /* device time of the persistent solver kernel */
     float finalize_ms;     /* device time of the FP64 finaliser */
+    float proposal_ms;     /* device time of the start proposal (-1 if none ran) */
+    int32_t kernel_launches; /* kernels the last fit call launched */
+    uint64_t fits_warm;    /* fits started from the proposal's parameters */
 } loc_stats;
 LOC_API int loc_last_stats(loc_ctx *ctx, loc_stats *stats);
 
@@ -285,6 +301,64 @@ LOC_API int loc_synth_frames(uint16_t *d_frames, int n_frames, int n_rows, int n
                              const float *d_emitters, const int *d_frame_start,
                              const float *d_background, float read_noise, unsigned long long seed,
                              void *stream);
+
+/*
+ * Learned start proposal (no reference counterpart: the reference starts
+ * every fit from the finder's centroid and the PSF width, Localization.cpp
+ * :122-142, 301-321, 466-491). A small convolutional network (1x11x11 window
+ * -> 3x3 convolutions with 16, 32, 32 channels -> linear head with one output
+ * per fit parameter) trained on synthetic windows labelled by the LM fit
+ * itself. Weights are FP32 masters; the two wide convolutions run on the
+ * tensor cores in BF16 with FP32 accumulation. Handles belong to one device.
+ */
+typedef struct loc_proposal loc_proposal;
+
+/* Weight count of the network for a method (its head has one output per
+ * parameter: 5, 4 or 7), or a negative error. */
+LOC_API int loc_proposal_weight_count(int method);
+/* New network with deterministic He-normal weights from `seed`. */
+LOC_API int loc_proposal_create(loc_proposal **net, int device, int method, unsigned long long seed);
+LOC_API int loc_proposal_destroy(loc_proposal *net);
+/* FP32 master weights, host buffers of loc_proposal_weight_count floats.
+ * Setting weights also resets the optimiser state. */
+LOC_API int loc_proposal_get_weights(loc_proposal *net, float *weights, int n);
+LOC_API int loc_proposal_set_weights(loc_proposal *net, const float *weights, int n);
+/*
+ * Raw head outputs for a stack of 11 x 11 uint16 windows (x fastest, window
+ * centre at (5, 5)): d_out receives n x P floats; d_index (optional) gathers
+ * window d_index[i] for row i; d_stat (optional) receives n x 2 floats of the
+ * window normalisation (border mean b0, scale s0). Device buffers.
+ */
+LOC_API int loc_proposal_forward(loc_proposal *net, const uint16_t *d_rois, const int *d_index, int n,
+                                 float *d_out, float *d_stat, void *stream);
+/*
+ * Training objective over a batch: mean over windows of sum_j lam[j] (o_j -
+ * t_j)^2, t the label mapped to the network's output scale (log amplitude /
+ * s0, log width / 1.5, position relative to the window centre, correlation,
+ * (offset - b0) / s0). d_labels: N x P floats in the method's parameter order
+ * with positions relative to the window centre, row d_index[i] used for
+ * window i; lam: P host floats. loc_proposal_gradient writes the gradient
+ * (weight layout) to d_grad and the loss to *loss; loc_proposal_train_step
+ * also applies one Adam step of learning rate lr.
+ */
+LOC_API int loc_proposal_gradient(loc_proposal *net, const uint16_t *d_rois, const int *d_index, int n,
+                                  const float *d_labels, const float *lam, float *d_grad, float *loss,
+                                  void *stream);
+LOC_API int loc_proposal_train_step(loc_proposal *net, const uint16_t *d_rois, const int *d_index, int n,
+                                    const float *d_labels, const float *lam, float lr, float *loss, void *stream);
+/* LOC_OK, or LOC_E_CUDA if a tensor-core wait in a proposal kernel ran out
+ * (the kernel then skipped its remaining work). */
+LOC_API int loc_proposal_status(loc_proposal *net);
+/*
+ * Synthetic training windows (11 x 11 uint16, x fastest) from the fit's
+ * forward model: one emitter within 1 px of the centre, widths U[1, 2] px
+ * (independent per axis if elliptic), amplitude lognormal (median 500,
+ * log-sd 0.6), background U[50, 200], Poisson(0.5) neighbours, Poisson +
+ * Gaussian read noise (sd 2). d_truth (optional): n x 6 floats (x, y,
+ * amplitude, sigma_x, sigma_y, background). No reference counterpart.
+ */
+LOC_API int loc_synth_rois(uint16_t *d_rois, int n, int elliptic, unsigned long long seed, float *d_truth,
+                           void *stream);
 
 /*
  * Compatibility entry points with the signatures of the reference DLL

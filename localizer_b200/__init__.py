@@ -50,7 +50,8 @@ class Options(C.Structure):
                 ("d_init_params", C.c_void_p), ("d_params_out", C.c_void_p), ("d_diag", C.c_void_p),
                 ("threads_per_fit", C.c_int32), ("tail_threads_per_fit", C.c_int32), ("level0_budget", C.c_int32),
                 ("fp64_rerun", C.c_int32), ("rerun_margin", C.c_float), ("rerun_pivot", C.c_float),
-                ("rerun_threads_per_fit", C.c_int32), ("serial_classes", C.c_int32)]
+                ("rerun_threads_per_fit", C.c_int32), ("serial_classes", C.c_int32),
+                ("proposal", C.c_void_p), ("warm_iter_limit", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -59,7 +60,8 @@ class Stats(C.Structure):
                                           "kcycles_step", "kcycles_pass", "kcycles_decide", "fits_fp64_rerun",
                                           "iterations_fp64_rerun", "kcycles_fp64_rerun",
                                           "kcycles_fp64_rerun_pass")] + \
-               [(n, C.c_float) for n in ("queue_ms", "solver_ms", "finalize_ms")]
+               [(n, C.c_float) for n in ("queue_ms", "solver_ms", "finalize_ms", "proposal_ms")] + \
+               [("kernel_launches", C.c_int32), ("fits_warm", C.c_uint64)]
 
     def as_dict(self):
         return {n: (float(getattr(self, n)) if n.endswith("_ms") else int(getattr(self, n)))
@@ -92,6 +94,19 @@ _PROTOS = {
     "LocalizerFitEmitters": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                        C.POINTER(C.c_int), C.POINTER(C.POINTER(C.c_double))]),
     "LocalizerFree": (None, [C.c_void_p]),
+    "loc_proposal_weight_count": (C.c_int, [C.c_int]),
+    "loc_proposal_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_ulonglong]),
+    "loc_proposal_destroy": (C.c_int, [C.c_void_p]),
+    "loc_proposal_get_weights": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "loc_proposal_set_weights": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "loc_proposal_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]),
+    "loc_proposal_gradient": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.POINTER(C.c_float), C.c_void_p]),
+    "loc_proposal_train_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                          C.c_float, C.POINTER(C.c_float), C.c_void_p]),
+    "loc_proposal_status": (C.c_int, [C.c_void_p]),
+    "loc_synth_rois": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_ulonglong, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

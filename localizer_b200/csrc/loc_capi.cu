@@ -66,7 +66,10 @@ struct loc_ctx {
     DevBuf frames, cands, out, flags;
     unsigned long long *stats_dev = nullptr;  // points into scratch of the last call
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_prop = nullptr;
     bool events_recorded = false;
+    bool warm_recorded = false;
+    int launches = 0;
     cudaStream_t aux[locb::kMaxAux] = {};
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[locb::kMaxAux] = {};
@@ -127,6 +130,7 @@ LOC_API int loc_ctx_create(loc_ctx **ctx, int device)
             return cuda_fail(e, "cudaEventCreate");
         }
     }
+    if ((e = cudaEventCreate(&c->ev_prop)) != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
     if ((e = cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming)) != cudaSuccess)
         return cuda_fail(e, "cudaEventCreate");
     for (int k = 0; k < locb::kMaxAux; ++k) {
@@ -149,6 +153,7 @@ LOC_API int loc_ctx_destroy(loc_ctx *ctx)
     ctx->flags.release();
     for (int k = 0; k < 4; ++k)
         if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
+    if (ctx->ev_prop) cudaEventDestroy(ctx->ev_prop);
     if (ctx->fork) cudaEventDestroy(ctx->fork);
     for (int k = 0; k < locb::kMaxAux; ++k) {
         if (ctx->aux[k]) cudaStreamDestroy(ctx->aux[k]);
@@ -187,11 +192,20 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
     const int rerun = o.fp64_rerun >= 0 ? 1 : 0;
-    const size_t need = locb::scratch_bytes(method, n_cands, o.precision, rerun);
+    locb::ProposalView prop{};
+    const bool warm = o.proposal != nullptr;
+    if (warm) {
+        locb::proposal_view(o.proposal, &prop);
+        if (prop.nout != locb::proposal_nout(method))
+            return fail(LOC_E_INVALID, "the proposal network was built for another method");
+        if (prop.device != ctx->device) return fail(LOC_E_INVALID, "the proposal network lives on another device");
+        if (o.precision == LOC_PRECISION_FP64) return fail(LOC_E_UNSUPPORTED, "start proposals run with FP32 solves");
+    }
+    const size_t need = locb::scratch_bytes(method, n_cands, o.precision, rerun, warm ? 1 : 0);
     e = ctx->scratch.ensure(need);
     if (e != cudaSuccess) return fail(LOC_E_NOMEM, std::string("scratch allocation: ") + cudaGetErrorString(e));
     locb::Scratch s;
-    locb::carve_scratch(ctx->scratch.p, method, n_cands, o.precision, rerun, &s);
+    locb::carve_scratch(ctx->scratch.p, method, n_cands, o.precision, rerun, &s, warm ? 1 : 0);
     locb::FitParams p{};
     p.frames = d_frames;
     p.n_frames = n_frames;
@@ -221,12 +235,19 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
         !(p.tail_threads_per_fit == 1 || p.tail_threads_per_fit == 4 || p.tail_threads_per_fit == 8))
         return fail(LOC_E_INVALID, "threads per fit must be 1, 4 or 8");
     p.init_params = o.d_init_params;
+    p.warm = warm;
+    p.prop = prop;
+    p.warm_iter_limit = o.warm_iter_limit == 0 ? 8 : (o.warm_iter_limit < 0 ? 0 : o.warm_iter_limit);
+    ctx->launches = 0;
+    p.launches = &ctx->launches;
     p.params_out = o.d_params_out;
     p.diag = o.d_diag;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing((cudaStream_t)stream, &cap);
     for (int k = 0; k < 4; ++k) p.ev[k] = cap == cudaStreamCaptureStatusNone ? ctx->ev[k] : nullptr;
     ctx->events_recorded = cap == cudaStreamCaptureStatusNone;
+    p.ev_prop = warm && cap == cudaStreamCaptureStatusNone ? ctx->ev_prop : nullptr;
+    ctx->warm_recorded = p.ev_prop != nullptr;
     for (int k = 0; k < locb::kMaxAux; ++k) {
         p.aux[k] = o.serial_classes ? nullptr : ctx->aux[k];
         p.join[k] = ctx->join[k];
@@ -259,7 +280,7 @@ LOC_API int loc_last_stats(loc_ctx *ctx, loc_stats *st)
         std::memset(st, 0, sizeof(*st));
         return LOC_OK;
     }
-    unsigned long long v[24];
+    unsigned long long v[locb::kStatWords];
     cudaError_t e = cudaMemcpy(v, ctx->stats_dev, sizeof(v), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(e, "stats copy");
     st->f_evals = v[0];
@@ -278,10 +299,17 @@ LOC_API int loc_last_stats(loc_ctx *ctx, loc_stats *st)
     st->iterations_fp64_rerun = v[12 + 5];
     st->kcycles_fp64_rerun = v[12 + 8] + v[12 + 9] + v[12 + 10] + v[12 + 11];
     st->kcycles_fp64_rerun_pass = v[12 + 10];
-    st->queue_ms = st->solver_ms = st->finalize_ms = -1.0f;
+    st->fits_warm = v[2 * 12];
+    st->kernel_launches = ctx->launches;
+    st->queue_ms = st->solver_ms = st->finalize_ms = st->proposal_ms = -1.0f;
     if (ctx->events_recorded && cudaEventSynchronize(ctx->ev[3]) == cudaSuccess) {
         cudaEventElapsedTime(&st->queue_ms, ctx->ev[0], ctx->ev[1]);
-        cudaEventElapsedTime(&st->solver_ms, ctx->ev[1], ctx->ev[2]);
+        if (ctx->warm_recorded) {
+            cudaEventElapsedTime(&st->proposal_ms, ctx->ev[1], ctx->ev_prop);
+            cudaEventElapsedTime(&st->solver_ms, ctx->ev_prop, ctx->ev[2]);
+        } else {
+            cudaEventElapsedTime(&st->solver_ms, ctx->ev[1], ctx->ev[2]);
+        }
         cudaEventElapsedTime(&st->finalize_ms, ctx->ev[2], ctx->ev[3]);
     }
     return LOC_OK;

@@ -169,8 +169,8 @@ __global__ void k3_flag(const float *state32, int stride, const int *cls, const 
 // appends the flagged fits to that class's FP64 queue (order2 / meta2).
 template <int P>
 __global__ void k3_flag_class(const float *state32, int stride, const int *order, const int *meta,
-                              const uint8_t *flags, int r, float margin, float pivot, int *cls2, int *order2,
-                              int *meta2)
+                              const uint8_t *flags, int r, float margin, float pivot, int warm_limit, int *cls2,
+                              int *order2, int *meta2)
 {
     using SL = StateLayout<P>;
     const int start = meta[m_start(r)], count = meta[m_count(r)];
@@ -180,8 +180,11 @@ __global__ void k3_flag_class(const float *state32, int stride, const int *order
         if (flags[i] != F_PENDING) continue;
         const float *s = state32 + (size_t)i * stride;
         const float status = s[SL::STATUS];
+        // warm-started fits (warm_limit > 0) that needed many iterations may
+        // stop elsewhere than the reference start's trajectory would
         const bool risky = status != (float)T_MAX_ITER &&
-                           (s[SL::MARGIN] < margin || s[SL::MINPIV] < pivot || status != 0.0f);
+                           (s[SL::MARGIN] < margin || s[SL::MINPIV] < pivot || status != 0.0f ||
+                            (warm_limit > 0 && s[SL::ITERS] > (float)warm_limit));
         if (risky) {
             cls2[i] = r;
             const int slot = atomicAdd(&meta2[m_count(r)], 1);
@@ -486,7 +489,7 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
                     minpiv_fit = T(1);
                     margin_fit = T(1e30);
                     esc_fit = 0;
-                    if (a.init_params) {
+                    if (a.init_params && !isnan(a.init_params[(size_t)my * P])) {
                         const float *ip = a.init_params + (size_t)my * P;
 #pragma unroll
                         for (int k = 0; k < P; ++k) {
@@ -1082,20 +1085,23 @@ namespace {
 size_t al256(size_t b) { return (b + 255) / 256 * 256; }
 }
 
-size_t scratch_bytes(int method, int n, int precision, int rerun)
+static_assert(kStatWords >= 2 * ST_N + 1, "statistics words");
+
+size_t scratch_bytes(int method, int n, int precision, int rerun, int warm)
 {
     const size_t el = precision == 1 ? sizeof(double) : sizeof(float);
     const int m = solver_method(method);
     size_t b = al256(sizeof(int) * (size_t)n) * 2 + al256(sizeof(int) * kMetaInts) +
-               al256(sizeof(unsigned long long) * 2 * ST_N) + al256(sizeof(int) * (size_t)n) +
+               al256(sizeof(unsigned long long) * kStatWords) + al256(sizeof(int) * (size_t)n) +
                al256(sizeof(float) * (size_t)n * cont_stride_of(m)) + al256(el * (size_t)n * state_stride(method));
     if (precision != 1 && rerun)
         b += al256(sizeof(int) * (size_t)n) * 2 + al256(sizeof(int) * kMetaInts) +
              al256(sizeof(double) * (size_t)n * state_stride(method));
+    if (warm) b += al256(sizeof(float) * (size_t)n * 8);
     return b;
 }
 
-void carve_scratch(void *base, int method, int n, int precision, int rerun, Scratch *s)
+void carve_scratch(void *base, int method, int n, int precision, int rerun, Scratch *s, int warm)
 {
     const size_t el = precision == 1 ? sizeof(double) : sizeof(float);
     char *p = (char *)base;
@@ -1106,7 +1112,7 @@ void carve_scratch(void *base, int method, int n, int precision, int rerun, Scra
     s->meta = (int *)p;
     p += al256(sizeof(int) * kMetaInts);
     s->stats = (unsigned long long *)p;
-    p += al256(sizeof(unsigned long long) * 2 * ST_N);
+    p += al256(sizeof(unsigned long long) * kStatWords);
     s->cont = (int *)p;
     p += al256(sizeof(int) * (size_t)n);
     s->cont_state = (float *)p;
@@ -1121,10 +1127,12 @@ void carve_scratch(void *base, int method, int n, int precision, int rerun, Scra
         s->meta2 = (int *)p;
         p += al256(sizeof(int) * kMetaInts);
         s->state64 = (double *)p;
+        p += al256(sizeof(double) * (size_t)n * state_stride(method));
     } else {
         s->cls2 = s->order2 = s->meta2 = nullptr;
         s->state64 = nullptr;
     }
+    s->init = warm ? (float *)p : nullptr;
 }
 
 namespace {
@@ -1147,6 +1155,7 @@ cudaError_t launch_queues(const FitParams &p, const K1Args &k1_in, const int *co
                        : launch_k1<7, T>(k1, r, tpb, p.blocks_per_sm, tpf, stream);
             if (e == cudaErrorInvalidValue) *err_detail = 1;
             if (e != cudaSuccess) return e;
+            if (p.launches) ++*p.launches;
         }
     }
     return e;
@@ -1165,7 +1174,7 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
     e = cudaMemsetAsync(s.meta, 0, sizeof(int) * kMetaInts, stream);
     if (e != cudaSuccess) return e;
     if (rerun && (e = cudaMemsetAsync(s.meta2, 0, sizeof(int) * kMetaInts, stream)) != cudaSuccess) return e;
-    e = cudaMemsetAsync(s.stats, 0, sizeof(unsigned long long) * 2 * ST_N, stream);
+    e = cudaMemsetAsync(s.stats, 0, sizeof(unsigned long long) * kStatWords, stream);
     if (e != cudaSuccess) return e;
     if (n == 0) {
         for (int k = 0; k < 4; ++k)
@@ -1178,6 +1187,9 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
     auto mark = [&](int k) {
         if (p.ev[k]) cudaEventRecord(p.ev[k], stream);
     };
+    auto bump = [&]() {
+        if (p.launches) ++*p.launches;
+    };
     mark(0);
     K0Args k0{(const Cand *)p.cands, n, p.n_frames, p.n_rows, p.n_cols, r_default, r_cap, p.method, ncol_total,
               p.out, p.flags, s.cls, s.meta, rerun ? s.cls2 : nullptr};
@@ -1186,6 +1198,9 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
     k0_classes<<<1, 32, 0, stream>>>(s.meta);
     k0_scatter<<<nb, 256, 0, stream>>>(s.cls, n, s.meta, s.order);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    bump();
+    bump();
+    bump();
 
     // which half-width queues exist: known bound from the caller, or the
     // histogram read back (one small synchronous copy)
@@ -1198,6 +1213,13 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
         if (e != cudaSuccess) return e;
     }
     mark(1);
+    // learned start proposal and start check, before the solver chains fork
+    if (p.warm) {
+        e = enqueue_proposal(p.prop, p.frames, (long long)p.n_rows * p.n_cols, p.n_rows, p.n_cols, p.cands, s.cls, n,
+                             p.method, (float)p.w0, s.init, s.stats + 2 * ST_N, p.prop.err, stream, p.launches);
+        if (e != cudaSuccess) return e;
+        if (p.ev_prop) cudaEventRecord(p.ev_prop, stream);
+    }
     int tpb = p.threads_per_block > 0 ? p.threads_per_block : 128;
     tpb = (tpb + 31) / 32 * 32;
     if (tpb > 128) tpb = 128;
@@ -1206,7 +1228,7 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
     K1Args k1{p.frames, (long long)p.n_rows * p.n_cols, p.n_rows, (const Cand *)p.cands, s.order, s.meta,
               s.state, state_stride(p.method), (float)p.w0, (float)(1.0 / (p.sigma * p.sigma)),
               (float)(1.0 / s_abs), 1.0 / (p.sigma * p.sigma), 1.0 / s_abs, p.max_iter, (float)p.epsabs,
-              (float)p.epsrel, p.precision == 1 ? 0.0f : p.pivot_thr, p.init_params, s.stats,
+              (float)p.epsrel, p.precision == 1 ? 0.0f : p.pivot_thr, p.warm ? s.init : p.init_params, s.stats,
               0, 0, s.cont, s.cont_state, cont_stride_of(m)};
     // Each ROI class is an independent chain -- level 0 (every candidate,
     // tpf0 threads per fit, up to `budget` iterations), level 1 (the fits
@@ -1243,19 +1265,23 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
             e = launch_queues<float>(p, k1, cnt1, r_cap, tpb, two_level, 0, cs, err_detail);
             if (e == cudaSuccess && rerun) {
                 const int fb = 2 * 148;
+                const int wl = p.warm ? p.warm_iter_limit : 0;
                 const float *st32 = (const float *)s.state;
                 const int sst = state_stride(p.method);
                 switch (m) {
                 case 0: k3_flag_class<5><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r, p.rerun_margin,
-                                                             p.rerun_pivot, s.cls2, s.order2, s.meta2); break;
+                                                             p.rerun_pivot, wl, s.cls2, s.order2, s.meta2); break;
                 case 1: k3_flag_class<4><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r, p.rerun_margin,
-                                                             p.rerun_pivot, s.cls2, s.order2, s.meta2); break;
+                                                             p.rerun_pivot, wl, s.cls2, s.order2, s.meta2); break;
                 default: k3_flag_class<7><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r,
-                                                              p.rerun_margin, p.rerun_pivot, s.cls2, s.order2,
+                                                              p.rerun_margin, p.rerun_pivot, wl, s.cls2, s.order2,
                                                               s.meta2); break;
                 }
                 if ((e = cudaGetLastError()) != cudaSuccess) return e;
+                bump();
                 K1Args k64 = k1;
+                // warm-started fits fall back to the reference start
+                if (p.warm) k64.init_params = nullptr;
                 k64.order = s.order2;
                 k64.meta = s.meta2;
                 k64.state = s.state64;
@@ -1278,6 +1304,7 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
               p.precision == 1 ? nullptr : (const float *)s.state,
               p.precision == 1 ? (const double *)s.state : s.state64, rerun ? s.cls2 : nullptr,
               state_stride(p.method), ncol_total, p.out, p.flags, p.params_out, p.diag};
+    bump();
     switch (p.method) {
     case 0: k2_finalize<0><<<nb, 256, 0, stream>>>(k2); break;
     case 1: k2_finalize<1><<<nb, 256, 0, stream>>>(k2); break;

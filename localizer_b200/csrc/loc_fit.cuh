@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "loc_proposal.cuh"
+
 namespace locb {
 
 constexpr int kMaxHalfWidth = 16;  // LOC_MAX_HALF_WIDTH
@@ -23,6 +25,7 @@ struct Scratch {
     int *order2;         // n: their queue
     int *meta2;          // kMetaInts: its class table
     double *state64;     // n * state_stride(method): FP64 state of re-run fits
+    float *init;         // n * P: proposed starts (warm mode only)
 };
 
 constexpr int kMetaInts = 8 + 8 * (kMaxHalfWidth + 1);
@@ -49,6 +52,11 @@ struct FitParams {
     float rerun_margin;        // branch-decision margin below which a fit is flagged
     float rerun_pivot;         // undamped pivot ratio below which a fit is flagged
     const float *init_params;
+    bool warm;                 // start proposal active (prop, warm_iter_limit)
+    ProposalView prop;
+    int warm_iter_limit;       // warm fits with more iterations are re-run from the reference start
+    cudaEvent_t ev_prop;       // optional: after the proposal kernel
+    int *launches;             // optional: incremented per kernel launch
     float *params_out;
     float *diag;
     cudaEvent_t ev[4];   // optional: before the queue build, around the solver, after the finaliser
@@ -60,8 +68,9 @@ struct FitParams {
 };
 
 int state_stride(int method);
-size_t scratch_bytes(int method, int n_cands, int precision, int rerun);
-void carve_scratch(void *base, int method, int n_cands, int precision, int rerun, Scratch *s);
+size_t scratch_bytes(int method, int n_cands, int precision, int rerun, int warm = 0);
+void carve_scratch(void *base, int method, int n_cands, int precision, int rerun, Scratch *s, int warm = 0);
+constexpr int kStatWords = 2 * 12 + 2;  // solver counters, FP64 re-run counters, proposals taken, spare
 
 // Enqueue the whole fit on `stream`. Returns cudaSuccess or the launch error;
 // *used_smem_side receives the ROI side the solver was sized for.

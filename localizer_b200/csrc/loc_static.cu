@@ -78,6 +78,7 @@ extern "C" LOC_API int loc_fit_batch_static(const uint16_t *d_frames, int n_fram
     else loc_default_options(&o);
     if (o.max_iter < 1) return err(LOC_E_INVALID, "max_iter < 1");
     if (!(o.epsrel >= 0) || !(o.epsabs >= 0)) return err(LOC_E_INVALID, "negative tolerance");
+    if (o.proposal) return err(LOC_E_UNSUPPORTED, "start proposals need a context (loc_fit_batch)");
     const int tpf0 = o.threads_per_fit > 0 ? o.threads_per_fit : 1;
     const int tpf1 = o.tail_threads_per_fit > 0 ? o.tail_threads_per_fit : 8;
     if (!(tpf0 == 1 || tpf0 == 4 || tpf0 == 8) || !(tpf1 == 1 || tpf1 == 4 || tpf1 == 8))
