@@ -11,7 +11,13 @@ Gaussian method (code 7) in one persistent FP32 solver launch per step.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 One JSON line on rank 0. A step = one fit call over every candidate of the
-stack (frames and candidates resident in HBM). `e2e` runs the same fit
+stack (frames and candidates resident in HBM). Two arms are timed on the same
+candidates: the plain LM (the reference's start values) and the
+learned-warm-start LM (a proposal network trained here on the GPU, before
+timing, on windows of separately seeded frames of the same workload; its
+cold-start fallback re-runs warm fits it judges unreliable with the
+reference start in FP64). `value` is the warm-start arm, as the metric names
+it; `plain_lm_fits_per_s` is the plain arm. `e2e` runs the warm-start fit
 through the host-buffer C-ABI call (loc_fit_host: frame and candidate upload
 from pinned host memory, fit, row and flag download) every step. The CPU
 reference arm runs the reference's own fitter (Localization.cpp compiled
@@ -65,7 +71,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -216,7 +222,7 @@ def reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames", type=int, default=10000)
@@ -224,6 +230,8 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=12.0, help="seconds of CPU work per reference step")
     ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--train-frames", type=int, default=4000, help="frames whose windows train the proposal")
+    ap.add_argument("--train-epochs", type=int, default=8)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -232,6 +240,7 @@ def main():
     import torch
 
     import localizer_b200 as L
+    from localizer_b200 import proposal as PR
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     if world > 1:
@@ -243,57 +252,84 @@ def main():
     n = len(cands)
     eng = L.Engine(local)
     ncol = L.lib().loc_output_columns(METHOD)
-    d_out = torch.empty((n, ncol), dtype=torch.float64, device="cuda")
-    d_flags = torch.empty(n, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
-    opts = L.default_options(max_half_width=int(max(w.half_widths)), precision=args.precision)
     n_frames, size = frames_dev.shape[0], frames_dev.shape[1]
 
-    def step():
+    # the proposal network, trained on the GPU by the library's own kernels
+    t_tr = time.time()
+    net, train_rep = PR.train(method=METHOD, n_rois=0, frames=args.train_frames, epochs=args.train_epochs,
+                              seed=7 + 1000 * rank, device=local)
+    train_rep["wall_s"] = time.time() - t_tr
+    log(f"[bench] rank {rank}: proposal trained in {train_rep['wall_s']:.1f}s "
+        f"({train_rep['labelled']} windows, holdout position median {train_rep['holdout_pos_median_px']:.3f} px)")
+    mh = int(max(w.half_widths))
+    arms = {"plain": L.default_options(max_half_width=mh, precision=args.precision),
+            "warm": L.default_options(max_half_width=mh, precision=args.precision, proposal=net.handle.value)}
+    outs = {k: (torch.empty((n, ncol), dtype=torch.float64, device="cuda"),
+                torch.empty(n, dtype=torch.uint8, device="cuda")) for k in arms}
+
+    def step(arm):
+        o, f = outs[arm]
         eng.fit_device(frames_dev.data_ptr(), n_frames, size, size, d_cands.data_ptr(), n, METHOD, w.w0, 1.0,
-                       d_out.data_ptr(), d_flags.data_ptr(), stream.cuda_stream, opts)
+                       o.data_ptr(), f.data_ptr(), stream.cuda_stream, arms[arm])
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    solver_ms, stats_last = [], None
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+    def timed(arm):
+        for _ in range(args.warmup):
+            step(arm)
         torch.cuda.synchronize()
-        start.record(stream)
-        for _ in range(args.steps):
-            step()
-            # per-stage device times of this step (events on the same stream)
-            stats_last = eng.stats()
-            solver_ms.append(stats_last["solver_ms"])
-        end.record(stream)
-        torch.cuda.synchronize()
-    elapsed_ms = start.elapsed_time(end)
-    t = torch.tensor([elapsed_ms], device="cuda")
-    if world > 1:
-        torch.distributed.barrier()
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        tot = torch.tensor([float(n)], device="cuda")
-        torch.distributed.all_reduce(tot)
-        total_fits = tot.item() * args.steps
-    else:
-        total_fits = float(n) * args.steps
-    elapsed_ms = t.item()
-    value = total_fits / (elapsed_ms / 1e3)
-    clocks = clk.summary()
+        if world > 1:
+            torch.distributed.barrier()
+        stage, stats_last = [], None
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            torch.cuda.synchronize()
+            start.record(stream)
+            for _ in range(args.steps):
+                step(arm)
+                # per-stage device times of this step (events on the same stream)
+                stats_last = eng.stats()
+                stage.append((stats_last["solver_ms"], stats_last["proposal_ms"]))
+            end.record(stream)
+            torch.cuda.synchronize()
+        t = torch.tensor([start.elapsed_time(end)], device="cuda")
+        if world > 1:
+            torch.distributed.barrier()
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            tot = torch.tensor([float(n)], device="cuda")
+            torch.distributed.all_reduce(tot)
+            total = tot.item() * args.steps
+        else:
+            total = float(n) * args.steps
+        ms = t.item()
+        return {"value": total / (ms / 1e3), "ms": ms, "stats": stats_last, "clocks": clk.summary(),
+                "solver_ms": float(np.mean([a for a, _ in stage])), "proposal_ms": float(np.mean([b for _, b in stage]))}
 
-    # roofline of the solver kernel: algorithmic FLOPs / kernel time vs FP32 peak
-    st = stats_last
+    res = {arm: timed(arm) for arm in ("plain", "warm")}
+    value = res["warm"]["value"]
+    elapsed_ms = res["warm"]["ms"]
+
+    # roofline of the plain solver: algorithmic FLOPs / solver time vs FP32 peak
+    st = res["plain"]["stats"]
+    clocks = res["warm"]["clocks"]
     p = NPAR[METHOD]
     flops = st["pixels_j"] * FLOP_J[METHOD] + st["pixels_f"] * FLOP_F + st["lambda_solves"] * (p ** 3 / 3 + 2 * p * p)
-    k_ms = float(np.mean(solver_ms))
+    k_ms = res["plain"]["solver_ms"]
     achieved = flops / (k_ms / 1e3) / 1e12
-    peak_mhz = clocks["sm_max_mhz"] or 1965.0
+    peak_mhz = res["plain"]["clocks"]["sm_max_mhz"] or 1965.0
     peak = SM_COUNT * FP32_LANES * 2 * peak_mhz * 1e6 / 1e12
+    # proposal network: algorithmic tensor-core FLOPs (valid conv2 + conv3
+    # outputs) per window over its device time vs the measured BF16 peak
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    bf16_peak = peaks.get("bf16_tflops", 1590.0)
+    prop_ms = res["warm"]["proposal_ms"]
+    tc_flops = n * 2.0 * (49 * 144 * 32 + 25 * 288 * 32)
+    prop_roof = {"bound": "tensor", "kernel": "k_prop_fwd", "achieved": tc_flops / (prop_ms / 1e3) / 1e12,
+                 "peak": bf16_peak, "unit": "TFLOP/s", "frac": tc_flops / (prop_ms / 1e3) / 1e12 / bf16_peak,
+                 "kernel_ms": prop_ms, "windows_per_s": n / (prop_ms / 1e3),
+                 "peak_source": "bf16_tflops of measured MEASURED_PEAKS.json" if peaks else "fallback 1.59 PFLOP/s"}
 
-    # e2e through the host-buffer C ABI call (pinned host memory), every rank
+    # e2e through the host-buffer C ABI call (pinned host memory), warm-start arm
     import ctypes as C
     lib = L.lib()
     ph_frames = torch.empty(frames_host.shape, dtype=torch.int16, pin_memory=True)
@@ -305,7 +341,7 @@ def main():
 
     def e2e_step():
         rc = lib.loc_fit_host(eng.handle, C.c_void_p(ph_frames.data_ptr()), n_frames, size, size,
-                              C.c_void_p(ph_cands.data_ptr()), n, METHOD, w.w0, 1.0, C.byref(opts),
+                              C.c_void_p(ph_cands.data_ptr()), n, METHOD, w.w0, 1.0, C.byref(arms["warm"]),
                               C.c_void_p(ph_out.data_ptr()), C.c_void_p(ph_flags.data_ptr()))
         if rc != 0:
             raise RuntimeError(lib.loc_last_error().decode())
@@ -324,35 +360,38 @@ def main():
     t2 = torch.tensor([s2.elapsed_time(e2) / args.e2e_steps], device="cuda")
     if world > 1:
         torch.distributed.all_reduce(t2, op=torch.distributed.ReduceOp.MAX)
+    total_fits = value * elapsed_ms / 1e3
     e2e = {"value": total_fits / args.steps / (t2.item() / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": int(frames_host.nbytes + cands.nbytes),
-           "d2h_bytes_per_step": int(n * ncol * 8 + n)}
+           "d2h_bytes_per_step": int(n * ncol * 8 + n), "arm": "warm"}
     rows_e2e = ph_out.numpy().copy()
     flags_e2e = ph_flags.numpy().copy()
 
-    # CPU reference on a bounded sample, and the accuracy of the GPU rows there
+    # CPU reference on a bounded sample, and the accuracy of both arms there
     cpu, accuracy = None, None
     if rank == 0 and not args.no_cpu_baseline:
         from oracle import oracle as O
-        rows_gpu = d_out.cpu().numpy()
-        flags_gpu = d_flags.cpu().numpy()
-        assert np.array_equal(rows_gpu[:, :ncol - 2], rows_e2e[:, :ncol - 2], equal_nan=True)
-        assert np.array_equal(flags_gpu, flags_e2e)
+        rows = {k: outs[k][0].cpu().numpy() for k in outs}
+        flg = {k: outs[k][1].cpu().numpy() for k in outs}
+        assert np.array_equal(rows["warm"][:, :ncol - 2], rows_e2e[:, :ncol - 2], equal_nan=True)
+        assert np.array_equal(flg["warm"], flags_e2e)
         if O.ref_available():
             v, ns, th, idx, rrows, rkept = run_reference_sample(frames_host, cands, w.w0, budget_s=args.ref_budget)
             cpu = {"value": v, "unit": UNIT, "cores": th, "kind": "reference",
                    "sample": f"{ns} candidates (whole frames spread through the stack); reference "
                              f"Localization.cpp FP64 + lmsder restatement, {th} host threads"}
-            g = rows_gpu[idx]
-            gk = flags_gpu[idx] == 0
-            both = gk & rkept
-            err = np.abs(g[both, 4:6] - rrows[both, 4:6]).max(axis=1)
-            accuracy = {"sample_fits": int(len(idx)), "flag_agreement": float(np.mean(gk == rkept)),
-                        "position_within_1e-3px": float(np.mean(err < 1e-3)) if len(err) else None,
-                        "position_max_err_px": float(err.max()) if len(err) else None,
-                        "reference": "reference fitter (FP64) on the same candidates"}
+            accuracy = {"sample_fits": int(len(idx)), "reference": "reference fitter (FP64) on the same candidates"}
+            for k in ("plain", "warm"):
+                g = rows[k][idx]
+                gk = flg[k][idx] == 0
+                both = gk & rkept
+                err = np.abs(g[both, 4:6] - rrows[both, 4:6]).max(axis=1)
+                accuracy[k] = {"flag_agreement": float(np.mean(gk == rkept)),
+                               "position_within_1e-3px": float(np.mean(err < 1e-3)) if len(err) else None,
+                               "position_max_err_px": float(err.max()) if len(err) else None}
 
     if rank == 0:
+        sw = res["warm"]["stats"]
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == 0 else "f64",
@@ -360,16 +399,28 @@ def main():
                 "config": {"workload": "batched uneven: 10000 frames 256x256 uint16, 20-400 emitters/frame, "
                                        "ellipsoidal PSF sigma U[1,2], ROI half-width in {3,4,5,6}, method 7",
                            "frames_per_gpu": n_frames, "candidates_per_gpu": n, "parallelism": f"dp{world}",
-                           "l2": "inputs larger than L2 (1.3 GB frames, 84 MB candidates, 300 MB rows)"},
-                "plain_lm_fits_per_s": value, "warm_start_lm_fits_per_s": None,
+                           "l2": "inputs larger than L2 (1.3 GB frames, 71 MB candidates, 256 MB rows)"},
+                "warm_start_lm_fits_per_s": value, "plain_lm_fits_per_s": res["plain"]["value"],
+                "warm_vs_plain": value / res["plain"]["value"],
+                "plain_ms_per_step": res["plain"]["ms"] / args.steps,
+                "warm_start": {"fits_warm": sw["fits_warm"], "fits_cold_fallback": sw["fits_fp64_rerun"],
+                               "iterations_per_fit": sw["iterations"] / max(sw["fits"], 1),
+                               "plain_iterations_per_fit": st["iterations"] / max(st["fits"], 1),
+                               "proposal_ms": prop_ms, "solver_ms": res["warm"]["solver_ms"],
+                               "training": train_rep},
                 "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                             "frac": achieved / peak, "traffic": None,
+                             "frac": achieved / peak, "traffic": 1537.0 * n,
+                             "traffic_note": "DRAM bytes per step of the level-0 FP32 solver, scaled from the "
+                                             "ncu capture of 1000 frames (1537 B per fit, r = 6 class)",
                              "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 x max SM clock); "
                                             "no measured FP32 peak in MEASURED_PEAKS.json",
-                             "kernel": "k1_lm_fit", "kernel_ms": k_ms, "flops_per_step": flops},
-                "stats": st, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu, "accuracy": accuracy,
-                "gpu_launches": 5 * args.steps}
+                             "kernel": "k1_lm_fit (plain arm, all classes and levels)", "kernel_ms": k_ms,
+                             "flops_per_step": flops},
+                "proposal_roofline": prop_roof,
+                "stats": sw, "plain_stats": st, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
+                "accuracy": accuracy, "gpu_launches": int(sw["kernel_launches"]) * args.steps}
         print(json.dumps(line))
+    net.close()
     eng.close()
     if world > 1:
         torch.distributed.destroy_process_group()

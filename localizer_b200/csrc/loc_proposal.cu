@@ -104,6 +104,8 @@ static_assert(kSmemFwd <= 227 * 1024, "forward kernel shared memory");
 static_assert(SO_ACT2 % 16 == 0 && SO_WP % 16 == 0 && SO_V % 16 == 0 && SO_BAR % 8 == 0, "alignment");
 
 constexpr uint32_t kIdesc = tc::idesc_bf16_f32<128, 32>();
+constexpr int kA3Stride = 808;   // floats per window of conv3 output in shared memory (800 + bank padding)
+static_assert(kR * kA3Stride * 4 <= 4 * (int)kLBO, "conv3 outputs fit in the conv2 activation buffer");
 
 // output roles: 0 amplitude, 1 width, 2 x, 3 y, 4 correlation, 5 offset
 template <int NOUT> __host__ __device__ constexpr int role(int j)
@@ -254,23 +256,36 @@ __global__ void __launch_bounds__(kThreads, 1) k_prop_fwd(FwdArgs a)
     for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
         const int base = g * kR;
         // ---- 1. windows (raw counts) ----
-        for (int k = tid; k < kR * kWin2; k += kThreads) {
-            const int rr = k / kWin2, px = k - rr * kWin2, jy = px / kWin, ix = px - jy * kWin;
-            const int item = base + rr;
-            float val = 0.f;
+        int *org = reinterpret_cast<int *>(stat);  // per window: x0, y0, frame (-1: none); stat is rewritten below
+        if (tid < kR) {
+            const int item = base + tid;
+            int x0 = 0, y0 = 0, fr = -1;
             if (item < a.n) {
                 if constexpr (MODE == 0) {
-                    const int src = a.index ? a.index[item] : item;
-                    val = (float)__ldg(a.rois + (size_t)src * kWin2 + px);
+                    fr = a.index ? a.index[item] : item;
+                } else if (a.cls[item] >= 0) {
+                    const Cand c = a.cands[item];
+                    x0 = (int)floor(c.x + 0.5) - 5;
+                    y0 = (int)floor(c.y + 0.5) - 5;
+                    fr = c.frame;
+                }
+            }
+            org[tid * 4 + 0] = x0;
+            org[tid * 4 + 1] = y0;
+            org[tid * 4 + 2] = fr;
+        }
+        __syncthreads();
+        for (int k = tid; k < kR * kWin2; k += kThreads) {
+            const int rr = k / kWin2, px = k - rr * kWin2, jy = px / kWin, ix = px - jy * kWin;
+            const int fr = org[rr * 4 + 2];
+            float val = 0.f;
+            if (fr >= 0) {
+                if constexpr (MODE == 0) {
+                    val = (float)__ldg(a.rois + (size_t)fr * kWin2 + px);
                 } else {
-                    if (a.cls[item] >= 0) {
-                        const Cand c = a.cands[item];
-                        const int cx = (int)floor(c.x + 0.5), cy = (int)floor(c.y + 0.5);
-                        const int xx = min(max(cx - 5 + ix, 0), a.n_rows - 1);
-                        const int yy = min(max(cy - 5 + jy, 0), a.n_cols - 1);
-                        val = (float)__ldg(a.frames + (size_t)c.frame * (size_t)a.frame_px + xx +
-                                           (size_t)yy * a.n_rows);
-                    }
+                    const int xx = min(max(org[rr * 4 + 0] + ix, 0), a.n_rows - 1);
+                    const int yy = min(max(org[rr * 4 + 1] + jy, 0), a.n_cols - 1);
+                    val = (float)__ldg(a.frames + (size_t)fr * (size_t)a.frame_px + xx + (size_t)yy * a.n_rows);
                 }
             }
             v[k] = val;
@@ -423,42 +438,59 @@ __global__ void __launch_bounds__(kThreads, 1) k_prop_fwd(FwdArgs a)
             break;
         }
         tc::fence_after_sync();
-        // ---- 7. conv3 epilogue: bias, ReLU, head partial sums ----
+        // ---- 7. conv3 epilogue: bias, ReLU -> a3 in shared memory (the
+        // activation buffers are free once the conv3 MMAs have completed) ----
+        float *a3s = reinterpret_cast<float *>(sm + SO_ACT2);   // [kR][kA3Stride], (channel, position)
         for (int i = 0; i < kTiles; ++i) {
             float acc[16];
             tc::tmem_ld16(tmem + t_lane + (uint32_t)(i * 32 + 16 * h), acc);
             tc::tmem_ld_wait();
             const int m = i * 128 + 32 * q + lane;
-            if (m < kRows) {
-                const int rr = m / 81, pos = m - rr * 81, oy = pos / 9, ox = pos - oy * 9;
-                if (oy < 5 && ox < 5) {
-                    const int p25 = oy * 5 + ox;
-                    float part[NOUT];
+            const int rr = m / 81, pos = m - rr * 81, oy = pos / 9, ox = pos - oy * 9;
+            if (m < kRows && oy < 5 && ox < 5) {
+                const int p25 = oy * 5 + ox;
 #pragma unroll
-                    for (int j = 0; j < NOUT; ++j) part[j] = 0.f;
+                for (int c = 0; c < 16; ++c) {
+                    const int ch = 16 * h + c;
+                    acc[c] = fmaxf(acc[c] + b23[32 + ch], 0.f);
+                    a3s[rr * kA3Stride + ch * 25 + p25] = acc[c];
+                }
+                if constexpr (MODE == 0) {
+                    if (a.save_a3 && base + rr < a.n) {
+                        float4 *d =
+                            reinterpret_cast<float4 *>(a.save_a3 + ((size_t)(base + rr) * 25 + p25) * 32 + 16 * h);
 #pragma unroll
-                    for (int c = 0; c < 16; ++c) {
-                        const int ch = 16 * h + c;
-                        const float a3 = fmaxf(acc[c] + b23[32 + ch], 0.f);
-                        acc[c] = a3;
-#pragma unroll
-                        for (int j = 0; j < NOUT; ++j) part[j] = fmaf(wh[(j * 32 + ch) * 25 + p25], a3, part[j]);
-                    }
-#pragma unroll
-                    for (int j = 0; j < NOUT; ++j) atomicAdd(&hacc[rr * 8 + j], part[j]);
-                    if constexpr (MODE == 0) {
-                        if (a.save_a3 && base + rr < a.n) {
-                            float4 *d = reinterpret_cast<float4 *>(a.save_a3 + ((size_t)(base + rr) * 25 + p25) * 32 +
-                                                                   16 * h);
-#pragma unroll
-                            for (int c = 0; c < 16; c += 4)
-                                d[c / 4] = make_float4(acc[c], acc[c + 1], acc[c + 2], acc[c + 3]);
-                        }
+                        for (int c = 0; c < 16; c += 4)
+                            d[c / 4] = make_float4(acc[c], acc[c + 1], acc[c + 2], acc[c + 3]);
                     }
                 }
             }
         }
         tc::fence_before_sync();
+        __syncthreads();
+        // ---- head: 16 threads per window, each over every 16th feature ----
+        {
+            static_assert(kThreads == 16 * kR, "head mapping");
+            const int rr = tid >> 4, sub = tid & 15;
+            const float *x = a3s + rr * kA3Stride;
+            float part[NOUT];
+#pragma unroll
+            for (int j = 0; j < NOUT; ++j) part[j] = 0.f;
+            for (int f = sub; f < 800; f += 16) {
+                const float xv = x[f];
+#pragma unroll
+                for (int j = 0; j < NOUT; ++j) part[j] = fmaf(wh[j * 800 + f], xv, part[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < NOUT; ++j) {
+                float t = part[j];
+                t += __shfl_xor_sync(0xffffffffu, t, 8);
+                t += __shfl_xor_sync(0xffffffffu, t, 4);
+                t += __shfl_xor_sync(0xffffffffu, t, 2);
+                t += __shfl_xor_sync(0xffffffffu, t, 1);
+                if (sub == 0) hacc[rr * 8 + j] = t;
+            }
+        }
         __syncthreads();
         // ---- 8. outputs ----
         if constexpr (MODE == 0) {

@@ -159,6 +159,77 @@ def label_rois(rois, method: int, w0: float = 1.5, engine: Engine | None = None)
     return labels, valid
 
 
+def frame_windows(frames, cands: np.ndarray, chunk: int = 1 << 18):
+    """11 x 11 windows (n, 121) int16 on the device, cut from a frame stack
+    (torch int16 (n_frames, n_cols, n_rows), [f, y, x]) around each
+    candidate's position rounded to the nearest pixel, edges clamped: the
+    windows the fit pipeline's proposal kernel sees."""
+    import torch
+    F, H, W = frames.shape
+    flat = frames.reshape(-1)
+    n = len(cands)
+    out = torch.empty((n, WINDOW * WINDOW), dtype=torch.int16, device=frames.device)
+    ar = torch.arange(WINDOW, device=frames.device)
+    for a in range(0, n, chunk):
+        c = cands[a:a + chunk]
+        x0 = torch.from_numpy(np.floor(c["x"] + 0.5).astype(np.int64) - 5).to(frames.device)
+        y0 = torch.from_numpy(np.floor(c["y"] + 0.5).astype(np.int64) - 5).to(frames.device)
+        fr = torch.from_numpy(c["frame"].astype(np.int64)).to(frames.device)
+        xs = (x0[:, None] + ar[None, :]).clamp(0, W - 1)
+        ys = (y0[:, None] + ar[None, :]).clamp(0, H - 1)
+        idx = fr[:, None, None] * (H * W) + ys[:, :, None] * W + xs[:, None, :]
+        out[a:a + len(c)] = torch.take(flat, idx.reshape(len(c), -1))
+    return out
+
+
+def frame_labels(frames, cands: np.ndarray, method: int, w0: float, engine: Engine | None = None):
+    """Plain LM fit of the candidates on their frames; labels (n, P) with
+    positions relative to the window centre (the rounded candidate
+    position), and the mask of kept fits."""
+    import torch
+    eng = engine or Engine(frames.device.index or 0)
+    F, H, W = frames.shape
+    n = len(cands)
+    nout = NOUT[method]
+    d_cands = torch.from_numpy(np.ascontiguousarray(cands).view(np.uint8)).cuda(frames.device)
+    ncol = _check(lib().loc_output_columns(method))
+    out = torch.empty((n, ncol), dtype=torch.float64, device=frames.device)
+    flags = torch.empty(n, dtype=torch.uint8, device=frames.device)
+    params = torch.empty((n, nout), dtype=torch.float32, device=frames.device)
+    rmax = int(cands["half_width"].max()) if n else 0
+    opts = default_options(max_half_width=rmax, d_params_out=params.data_ptr())
+    eng.fit_device(frames.data_ptr(), F, W, H, d_cands.data_ptr(), n, method, w0, 1.0, out.data_ptr(),
+                   flags.data_ptr(), 0, opts)
+    eng.sync(0)
+    roles = ROLES[nout]
+    cx = torch.from_numpy(np.floor(cands["x"] + 0.5)).float().to(frames.device)
+    cy = torch.from_numpy(np.floor(cands["y"] + 0.5)).float().to(frames.device)
+    labels = params.clone()
+    labels[:, roles.index(2)] -= cx
+    labels[:, roles.index(3)] -= cy
+    valid = (flags == 0) & torch.isfinite(labels).all(dim=1)
+    if engine is None:
+        eng.close()
+    return labels, valid
+
+
+def workload_windows(n_frames: int, method: int, seed: int, pfa: float = 30.0):
+    """Windows cut from synthetic frames of the batched uneven workload type
+    (seeded, disjoint from the evaluation seeds), labelled by the plain LM
+    fit of their candidates at the candidates' own ROI half-widths."""
+    from . import find_candidates
+    from . import synth
+    w = synth.scaled(synth.workloads()["uneven"], n_frames, seed=seed)
+    frames, _ = synth.make_device(w)
+    host = frames.cpu().numpy().view(np.uint16)
+    cands = find_candidates(host, pfa, w.w0)
+    cands["half_width"] = np.random.default_rng(seed + 17).choice(np.array(w.half_widths), size=len(cands))
+    labels, valid = frame_labels(frames, cands, method, w.w0)
+    rois = frame_windows(frames, cands)
+    del frames
+    return rois, labels, valid
+
+
 def window_stats(rois_np: np.ndarray):
     """Border mean b0 and scale s0 of each window (the network's normalisation)."""
     w = rois_np.astype(np.float64).reshape(-1, WINDOW, WINDOW)
@@ -191,13 +262,26 @@ def to_params(out: np.ndarray, b0: np.ndarray, s0: np.ndarray, nout: int) -> np.
 
 
 def train(method: int = 7, n_rois: int = 2_000_000, epochs: int = 8, batch: int = 4096, lr: float = 2e-3,
-          seed: int = 7, device: int = 0, holdout: float = 0.02, log=None):
-    """Generate, label and train. Returns (Proposal, report dict)."""
+          seed: int = 7, device: int = 0, holdout: float = 0.02, log=None, frames: int = 0):
+    """Generate, label and train. Windows: n_rois isolated synthetic windows
+    (loc_synth_rois), plus, if frames > 0, the candidates' windows of that
+    many synthetic frames of the batched uneven workload. Returns
+    (Proposal, report dict)."""
     import torch
     t0 = time.time()
     nout = NOUT[method]
-    rois = synth_rois(n_rois, elliptic=method in (5, 7), seed=seed)
-    labels, valid = label_rois(rois, method)
+    parts_r, parts_l, parts_v = [], [], []
+    if n_rois > 0:
+        r = synth_rois(n_rois, elliptic=method in (5, 7), seed=seed)
+        lab, val = label_rois(r, method)
+        parts_r.append(r); parts_l.append(lab); parts_v.append(val)
+    if frames > 0:
+        r, lab, val = workload_windows(frames, method, seed=100_000 + seed)
+        parts_r.append(r); parts_l.append(lab); parts_v.append(val)
+    rois = torch.cat(parts_r) if len(parts_r) > 1 else parts_r[0]
+    labels = torch.cat(parts_l) if len(parts_l) > 1 else parts_l[0]
+    valid = torch.cat(parts_v) if len(parts_v) > 1 else parts_v[0]
+    n_rois = rois.shape[0]
     torch.cuda.synchronize()
     t_data = time.time() - t0
     idx_all = torch.nonzero(valid).flatten().to(torch.int32)
