@@ -303,6 +303,20 @@ LOC_API int loc_synth_frames(uint16_t *d_frames, int n_frames, int n_rows, int n
                              void *stream);
 
 /*
+ * GLRT + adjacent-8 candidate finder on the GPU (reference
+ * ThresholdImage_GLRT_FFT, source/Segmentation.cpp:241-430, and
+ * ParticleFinder_adjacent8, source/ParticleFinding.cpp:283-427), with the
+ * same results, bit for bit and in the same order, as
+ * loc_find_candidates_host. d_frames: device frame stack (x fastest);
+ * d_cands: device array receiving up to max_cands candidates in frame order
+ * (half_width 0). Returns the total number found (which may exceed
+ * max_cands: call again with a larger buffer), or a negative error. Blocks
+ * until the candidates are written. PSF widths up to 8 px (window <= 33).
+ */
+LOC_API long loc_find_candidates(const uint16_t *d_frames, int n_frames, int n_rows, int n_cols, double pfa,
+                                 double psf_width, loc_candidate *d_cands, long max_cands, void *stream);
+
+/*
  * Learned start proposal (no reference counterpart: the reference starts
  * every fit from the finder's centroid and the PSF width, Localization.cpp
  * :122-142, 301-321, 466-491). A small convolutional network (1x11x11 window

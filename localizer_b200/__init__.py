@@ -94,6 +94,8 @@ _PROTOS = {
     "LocalizerFitEmitters": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                        C.POINTER(C.c_int), C.POINTER(C.POINTER(C.c_double))]),
     "LocalizerFree": (None, [C.c_void_p]),
+    "loc_find_candidates": (C.c_long, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p,
+                                       C.c_long, C.c_void_p]),
     "loc_proposal_weight_count": (C.c_int, [C.c_int]),
     "loc_proposal_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_ulonglong]),
     "loc_proposal_destroy": (C.c_int, [C.c_void_p]),
@@ -257,6 +259,23 @@ def find_candidates(frames: np.ndarray, pfa: float, psf_width: float, n_threads:
                                                   n_threads, out.ctypes.data, cap))
         if n <= cap:
             return out[:n].copy()
+        cap = n
+
+
+def find_candidates_device(frames, pfa: float, psf_width: float, stream: int = 0):
+    """GLRT + adjacent-8 candidates on the GPU for a device frame stack
+    (torch int16/uint16 tensor (n_frames, n_cols, n_rows), [f, y, x]).
+    Returns (device uint8 tensor of n * 40 bytes, n); identical to
+    find_candidates on the same frames."""
+    import torch
+    n_frames, n_cols, n_rows = frames.shape
+    cap = max(1024, n_frames * 64)
+    while True:
+        out = torch.empty(cap * CANDIDATE_DTYPE.itemsize, dtype=torch.uint8, device=frames.device)
+        n = _check(lib().loc_find_candidates(C.c_void_p(frames.data_ptr()), n_frames, n_rows, n_cols, pfa,
+                                             psf_width, C.c_void_p(out.data_ptr()), cap, C.c_void_p(stream)))
+        if n <= cap:
+            return out[:n * CANDIDATE_DTYPE.itemsize], n
         cap = n
 
 
