@@ -127,14 +127,25 @@ def make_workload(n_frames: int, rank: int):
     frames_dev, em = synth.make_device(w)
     frames_host = frames_dev.cpu().numpy().view(np.uint16)
     t1 = time.time()
-    cands = L.find_candidates(frames_host, PFA, w.w0)
+    # candidates from the GPU GLRT + adjacent-8 finder (bit-exact with the
+    # host finder), timed with CUDA events on its second run
+    L.find_candidates_device(frames_dev, PFA, w.w0)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    raw, n = L.find_candidates_device(frames_dev, PFA, w.w0)
+    e.record()
+    torch.cuda.synchronize()
+    f_ms = s.elapsed_time(e)
+    cands = raw.cpu().numpy().view(L.CANDIDATE_DTYPE).copy()
     rng = np.random.default_rng(w.seed + 17)
     cands["half_width"] = rng.choice(np.array(w.half_widths), size=len(cands))
-    t2 = time.time()
-    log(f"[bench] rank {rank}: {n_frames} frames rendered in {t1 - t0:.1f}s, {len(cands)} candidates found in "
-        f"{t2 - t1:.1f}s")
+    finder = {"ms": f_ms, "frames_per_s": n_frames / (f_ms / 1e3), "candidates": int(n),
+              "frame_read_gbs": frames_host.nbytes / (f_ms / 1e3) / 1e9,
+              "kernels": "k_glrt, k_union, k_flatten, k_count_roots, k_assign, k_accumulate, k_emit"}
+    log(f"[bench] rank {rank}: {n_frames} frames rendered in {t1 - t0:.1f}s, {len(cands)} candidates found on the "
+        f"GPU in {f_ms:.1f} ms")
     d_cands = torch.from_numpy(cands.view(np.uint8)).cuda()
-    return w, frames_dev, frames_host, cands, d_cands
+    return w, frames_dev, frames_host, cands, d_cands, finder
 
 
 def run_reference_sample(frames_host, cands, w0, budget_s=12.0, threads=None):
@@ -197,7 +208,7 @@ def reference_arm(args):
         return 0
     import torch
     torch.cuda.set_device(local)
-    w, frames_dev, frames_host, cands, d_cands = make_workload(args.frames, 0)
+    w, frames_dev, frames_host, cands, d_cands, _ = make_workload(args.frames, 0)
     vals = []
     for step in range(args.warmup + args.steps):
         v, n, th, _, _, _ = run_reference_sample(frames_host, cands, w.w0, budget_s=args.ref_budget)
@@ -248,7 +259,7 @@ def main():
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    w, frames_dev, frames_host, cands, d_cands = make_workload(args.frames, rank)
+    w, frames_dev, frames_host, cands, d_cands, finder = make_workload(args.frames, rank)
     n = len(cands)
     eng = L.Engine(local)
     ncol = L.lib().loc_output_columns(METHOD)
@@ -416,7 +427,7 @@ def main():
                                             "no measured FP32 peak in MEASURED_PEAKS.json",
                              "kernel": "k1_lm_fit (plain arm, all classes and levels)", "kernel_ms": k_ms,
                              "flops_per_step": flops},
-                "proposal_roofline": prop_roof,
+                "proposal_roofline": prop_roof, "finder": finder,
                 "stats": sw, "plain_stats": st, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
                 "accuracy": accuracy, "gpu_launches": int(sw["kernel_launches"]) * args.steps}
         print(json.dumps(line))
