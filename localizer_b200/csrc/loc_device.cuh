@@ -400,17 +400,21 @@ __device__ __forceinline__ int chol_solve(const MS (&Ms)[tri(P)], MS par, const 
 {
     T L[tri(P)];
     T inv[P];
-    T mp = T(1);
+    // smallest pivot ratio d / djj, kept as a fraction (one division at the
+    // end instead of one per pivot: FP64 division is long-latency)
+    T mpn = T(1), mpd = T(1);
 #pragma unroll
     for (int j = 0; j < P; ++j) {
         const T djj = (T)Ms[pku(P, j, j)] + (T)par;
         T d = djj;
 #pragma unroll
         for (int k = 0; k < j; ++k) d -= L[pkl(j, k)] * L[pkl(j, k)];
-        const T ratio = d / djj;
-        mp = ratio < mp ? ratio : mp;
+        if (d * mpd < mpn * djj) {
+            mpn = d;
+            mpd = djj;
+        }
         if (!(d > thr * djj)) {
-            minpiv = (MS)mp;
+            minpiv = (MS)(mpn / mpd);
             return thr > T(0) ? 1 : 2;
         }
         const T il = frsqrt(d);
@@ -424,7 +428,7 @@ __device__ __forceinline__ int chol_solve(const MS (&Ms)[tri(P)], MS par, const 
             L[pkl(i, j)] = sacc * inv[j];
         }
     }
-    minpiv = (MS)mp;
+    minpiv = (MS)(mpn / mpd);
     T y[P];
 #pragma unroll
     for (int i = 0; i < P; ++i) {
