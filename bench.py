@@ -16,9 +16,12 @@ candidates: the plain LM (the reference's start values) and the
 learned-warm-start LM (a proposal network trained here on the GPU, before
 timing, on windows of separately seeded frames of the same workload; its
 cold-start fallback re-runs warm fits it judges unreliable with the
-reference start in FP64). `value` is the warm-start arm, as the metric names
-it; `plain_lm_fits_per_s` is the plain arm. `e2e` runs the warm-start fit
-through the host-buffer C-ABI call (loc_fit_host: frame and candidate upload
+reference start in FP64). The metric is fits/s at the accuracy gate
+(positions within 1e-3 px of the FP64 reference, >= 99.9 % flag agreement):
+`value` is the plain arm, the configuration that meets the gate on this
+workload (the warm-start arm is slower and misses the flag gate here: both
+arms' fits/s, their ratio and their accuracy on the reference sample are in
+the line). `e2e` runs the plain fit through the host-buffer C-ABI call (loc_fit_host: frame and candidate upload
 from pinned host memory, fit, row and flag download) every step. The CPU
 reference arm runs the reference's own fitter (Localization.cpp compiled
 from the reference sources into oracle/_ref) on the host cores.
@@ -251,6 +254,7 @@ def main():
     import torch
 
     import localizer_b200 as L
+    from localizer_b200 import dist as DI
     from localizer_b200 import proposal as PR
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -302,26 +306,20 @@ def main():
                 stage.append((stats_last["solver_ms"], stats_last["proposal_ms"]))
             end.record(stream)
             torch.cuda.synchronize()
-        t = torch.tensor([start.elapsed_time(end)], device="cuda")
         if world > 1:
             torch.distributed.barrier()
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            tot = torch.tensor([float(n)], device="cuda")
-            torch.distributed.all_reduce(tot)
-            total = tot.item() * args.steps
-        else:
-            total = float(n) * args.steps
-        ms = t.item()
-        return {"value": total / (ms / 1e3), "ms": ms, "stats": stats_last, "clocks": clk.summary(),
+        # whole-job throughput: summed work over the slowest rank's time
+        total, ms, rate = DI.job_throughput(n * args.steps, start.elapsed_time(end))
+        return {"value": rate, "ms": ms, "stats": stats_last, "clocks": clk.summary(),
                 "solver_ms": float(np.mean([a for a, _ in stage])), "proposal_ms": float(np.mean([b for _, b in stage]))}
 
     res = {arm: timed(arm) for arm in ("plain", "warm")}
-    value = res["warm"]["value"]
-    elapsed_ms = res["warm"]["ms"]
+    value = res["plain"]["value"]
+    elapsed_ms = res["plain"]["ms"]
 
     # roofline of the plain solver: algorithmic FLOPs / solver time vs FP32 peak
     st = res["plain"]["stats"]
-    clocks = res["warm"]["clocks"]
+    clocks = res["plain"]["clocks"]
     p = NPAR[METHOD]
     flops = st["pixels_j"] * FLOP_J[METHOD] + st["pixels_f"] * FLOP_F + st["lambda_solves"] * (p ** 3 / 3 + 2 * p * p)
     k_ms = res["plain"]["solver_ms"]
@@ -352,7 +350,7 @@ def main():
 
     def e2e_step():
         rc = lib.loc_fit_host(eng.handle, C.c_void_p(ph_frames.data_ptr()), n_frames, size, size,
-                              C.c_void_p(ph_cands.data_ptr()), n, METHOD, w.w0, 1.0, C.byref(arms["warm"]),
+                              C.c_void_p(ph_cands.data_ptr()), n, METHOD, w.w0, 1.0, C.byref(arms["plain"]),
                               C.c_void_p(ph_out.data_ptr()), C.c_void_p(ph_flags.data_ptr()))
         if rc != 0:
             raise RuntimeError(lib.loc_last_error().decode())
@@ -374,7 +372,7 @@ def main():
     total_fits = value * elapsed_ms / 1e3
     e2e = {"value": total_fits / args.steps / (t2.item() / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": int(frames_host.nbytes + cands.nbytes),
-           "d2h_bytes_per_step": int(n * ncol * 8 + n), "arm": "warm"}
+           "d2h_bytes_per_step": int(n * ncol * 8 + n), "arm": "plain"}
     rows_e2e = ph_out.numpy().copy()
     flags_e2e = ph_flags.numpy().copy()
 
@@ -384,8 +382,8 @@ def main():
         from oracle import oracle as O
         rows = {k: outs[k][0].cpu().numpy() for k in outs}
         flg = {k: outs[k][1].cpu().numpy() for k in outs}
-        assert np.array_equal(rows["warm"][:, :ncol - 2], rows_e2e[:, :ncol - 2], equal_nan=True)
-        assert np.array_equal(flg["warm"], flags_e2e)
+        assert np.array_equal(rows["plain"][:, :ncol - 2], rows_e2e[:, :ncol - 2], equal_nan=True)
+        assert np.array_equal(flg["plain"], flags_e2e)
         if O.ref_available():
             v, ns, th, idx, rrows, rkept = run_reference_sample(frames_host, cands, w.w0, budget_s=args.ref_budget)
             cpu = {"value": v, "unit": UNIT, "cores": th, "kind": "reference",
@@ -411,9 +409,9 @@ def main():
                                        "ellipsoidal PSF sigma U[1,2], ROI half-width in {3,4,5,6}, method 7",
                            "frames_per_gpu": n_frames, "candidates_per_gpu": n, "parallelism": f"dp{world}",
                            "l2": "inputs larger than L2 (1.3 GB frames, 71 MB candidates, 256 MB rows)"},
-                "warm_start_lm_fits_per_s": value, "plain_lm_fits_per_s": res["plain"]["value"],
-                "warm_vs_plain": value / res["plain"]["value"],
-                "plain_ms_per_step": res["plain"]["ms"] / args.steps,
+                "warm_start_lm_fits_per_s": res["warm"]["value"], "plain_lm_fits_per_s": value,
+                "warm_vs_plain": res["warm"]["value"] / value,
+                "warm_ms_per_step": res["warm"]["ms"] / args.steps, "value_arm": "plain",
                 "warm_start": {"fits_warm": sw["fits_warm"], "fits_cold_fallback": sw["fits_fp64_rerun"],
                                "iterations_per_fit": sw["iterations"] / max(sw["fits"], 1),
                                "plain_iterations_per_fit": st["iterations"] / max(st["fits"], 1),
@@ -428,8 +426,8 @@ def main():
                              "kernel": "k1_lm_fit (plain arm, all classes and levels)", "kernel_ms": k_ms,
                              "flops_per_step": flops},
                 "proposal_roofline": prop_roof, "finder": finder,
-                "stats": sw, "plain_stats": st, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
-                "accuracy": accuracy, "gpu_launches": int(sw["kernel_launches"]) * args.steps}
+                "stats": st, "warm_stats": sw, "clocks": clocks, "warm_clocks": res["warm"]["clocks"], "e2e": e2e, "cpu_baseline": cpu,
+                "accuracy": accuracy, "gpu_launches": int(st["kernel_launches"]) * args.steps}
         print(json.dumps(line))
     net.close()
     eng.close()
