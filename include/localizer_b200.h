@@ -303,6 +303,20 @@ LOC_API int loc_synth_frames(uint16_t *d_frames, int n_frames, int n_rows, int n
                              void *stream);
 
 /*
+ * Text file of the kept positions in the reference's format
+ * (LocalizedPositionsContainer_*::writePositionsToFile, reference
+ * source/Storage.cpp:292-345, 427-470, 642-700): title line, `header`, "DATA
+ * FOLLOWS", column titles, one tab-separated line per row whose flag is 0 (all
+ * rows if flags is NULL), in row order. rows: n host rows as the fit calls
+ * write them (loc_output_columns(method) doubles). Byte-identical to the
+ * reference's file for the same positions. Returns the number of positions
+ * written; LOC_E_INVALID if none is kept (the reference throws "No
+ * positions localized!") or the file cannot be written.
+ */
+LOC_API long loc_write_positions_text(const double *rows, const uint8_t *flags, long n, int method,
+                                      const char *path, const char *header);
+
+/*
  * GLRT + adjacent-8 candidate finder on the GPU (reference
  * ThresholdImage_GLRT_FFT, source/Segmentation.cpp:241-430, and
  * ParticleFinder_adjacent8, source/ParticleFinding.cpp:283-427), with the

@@ -94,6 +94,7 @@ _PROTOS = {
     "LocalizerFitEmitters": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                        C.POINTER(C.c_int), C.POINTER(C.POINTER(C.c_double))]),
     "LocalizerFree": (None, [C.c_void_p]),
+    "loc_write_positions_text": (C.c_long, [C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_char_p, C.c_char_p]),
     "loc_find_candidates": (C.c_long, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p,
                                        C.c_long, C.c_void_p]),
     "loc_proposal_weight_count": (C.c_int, [C.c_int]),
@@ -277,6 +278,16 @@ def find_candidates_device(frames, pfa: float, psf_width: float, stream: int = 0
         if n <= cap:
             return out[:n * CANDIDATE_DTYPE.itemsize], n
         cap = n
+
+
+def write_positions(path: str, rows: np.ndarray, flags: np.ndarray | None, method: int, header: str = "") -> int:
+    """Write the kept rows as the reference's localized-positions text file
+    (loc_write_positions_text); returns the number of positions written."""
+    rows = np.ascontiguousarray(rows, dtype=np.float64)
+    n = rows.shape[0]
+    fl = None if flags is None else np.ascontiguousarray(flags, dtype=np.uint8)
+    return _check(lib().loc_write_positions_text(rows.ctypes.data, fl.ctypes.data if fl is not None else None, n,
+                                                 method, path.encode(), header.encode()))
 
 
 class LocalizedPositions:

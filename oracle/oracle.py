@@ -85,6 +85,9 @@ def ref():
                               C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ref_find_adjacent8.restype = C.c_int
         L.ref_find_adjacent8.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+        L.ref_write_positions.restype = C.c_int
+        L.ref_write_positions.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                          C.c_double, C.c_double, C.c_char_p, C.c_char_p]
         _ref = L
     return _ref
 
@@ -217,3 +220,15 @@ def ref_fit(frames, cands, method, w0, sigma=1.0):
     inv = np.empty_like(order)
     inv[order] = np.arange(nc)
     return out[inv], kept[inv], iters[inv], status[inv]
+
+
+def ref_write_positions(frames, cands, method, w0, path, header="", sigma=1.0):
+    """The reference's own writePositionsToFile for one frame's candidates
+    (same frame and ROI half-width). Returns the number of positions."""
+    n_frames, n_rows, n_cols = _stack_dims(frames)
+    cands = np.ascontiguousarray(cands, dtype=CAND_DTYPE)
+    rc = ref().ref_write_positions(frames.ctypes.data, n_frames, n_rows, n_cols, cands.ctypes.data, len(cands),
+                                   method, w0, sigma, path.encode(), header.encode())
+    if rc < 0:
+        raise RuntimeError(f"ref_write_positions failed: {rc}")
+    return rc

@@ -218,6 +218,46 @@ int ref_fit(const uint16_t *frames, int n_frames, int n_rows, int n_cols, const 
     return 0;
 }
 
+/*
+ * The reference's own text writer: fit one frame's candidates (all with the
+ * same frame and ROI half-width) with the reference fitter of `method`, set
+ * the frame numbers as the controller does (PALMAnalysis.cpp:238) and write
+ * them with writePositionsToFile (Storage.cpp:292-345, 427-470, 642-700).
+ * Returns the number of positions written, or a negative code.
+ */
+int ref_write_positions(const uint16_t *frames, int n_frames, int n_rows, int n_cols, const void *cands_v, int nc,
+                        int method, double w0, double sigma, const char *path, const char *header)
+{
+    const Cand *cands = (const Cand *)cands_v;
+    if (nc <= 0) return -2;
+    for (int i = 1; i < nc; i++)
+        if (cands[i].frame != cands[0].frame || cands[i].half_width != cands[0].half_width) return -2;
+    const int fr = cands[0].frame;
+    if (fr < 0 || fr >= n_frames) return -2;
+    /* make sure the stream library (and its locale) of this library is set up */
+    static std::ios_base::Init ios_init;
+    try {
+        size_t r = cands[0].half_width > 0 ? (size_t)cands[0].half_width : (size_t)std::ceil(w0 * 4.0);
+        ImagePtr img = frame_image(frames, fr, n_rows, n_cols);
+        auto lst = std::make_shared<std::list<Particle>>();
+        for (int i = 0; i < nc; i++) {
+            Particle p;
+            p.x = cands[i].x;
+            p.y = cands[i].y;
+            p.intensity = cands[i].intensity;
+            p.background = cands[i].background;
+            lst->push_back(p);
+        }
+        auto fitter = make_fitter(method, w0, sigma, r);
+        auto res = fitter->fit_positions(img, lst);
+        res->setFrameNumbers((size_t)fr);
+        res->writePositionsToFile(std::string(path), std::string(header));
+        return (int)res->getNPositions();
+    } catch (...) {
+        return -1;
+    }
+}
+
 /* The reference's adjacent-8 finder on a given mask (255 = detected). */
 int ref_find_adjacent8(const uint16_t *frame, int n_rows, int n_cols, const int32_t *mask,
                        double *out, int max_out)
