@@ -303,6 +303,22 @@ LOC_API int loc_synth_frames(uint16_t *d_frames, int n_frames, int n_rows, int n
                              void *stream);
 
 /*
+ * Frame ingest (reference BufferWithFormatToImage / CopyBufferToImage,
+ * source/FileIO.cpp:195-234, FileIO.h:96-116): n_frames camera buffers of
+ * storage type `format` (the reference's LocalizerStorageType codes,
+ * source/Defines.h:82-95: 2 int8, 3 uint8, 4 int16, 5 uint16, 6 int32,
+ * 7 uint32, 8 int64, 9 uint64, 10 float, 11 double; the 4-bit types are not
+ * supported), each n_rows x n_cols and column-major (row_major = 0, element
+ * (i, j) at i + j * n_rows) or row-major (1, at i * n_cols + j), to the fit
+ * path's uint16 stack. Values are rounded to the nearest integer and clamped
+ * to [0, 65535]; returns the number of pixels whose value that changed (0:
+ * lossless, as for 8/16-bit unsigned cameras), or a negative error. Device
+ * buffers; blocks until done.
+ */
+LOC_API long long loc_ingest_frames(const void *d_src, int format, int n_frames, int n_rows, int n_cols,
+                                    int row_major, uint16_t *d_dst, void *stream);
+
+/*
  * Text file of the kept positions in the reference's format
  * (LocalizedPositionsContainer_*::writePositionsToFile, reference
  * source/Storage.cpp:292-345, 427-470, 642-700): title line, `header`, "DATA

@@ -94,6 +94,8 @@ _PROTOS = {
     "LocalizerFitEmitters": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                        C.POINTER(C.c_int), C.POINTER(C.POINTER(C.c_double))]),
     "LocalizerFree": (None, [C.c_void_p]),
+    "loc_ingest_frames": (C.c_longlong, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                         C.c_void_p]),
     "loc_write_positions_text": (C.c_long, [C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_char_p, C.c_char_p]),
     "loc_find_candidates": (C.c_long, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p,
                                        C.c_long, C.c_void_p]),
@@ -278,6 +280,28 @@ def find_candidates_device(frames, pfa: float, psf_width: float, stream: int = 0
         if n <= cap:
             return out[:n * CANDIDATE_DTYPE.itemsize], n
         cap = n
+
+
+STORAGE_FORMATS = {"int8": 2, "uint8": 3, "int16": 4, "uint16": 5, "int32": 6, "uint32": 7, "int64": 8,
+                   "uint64": 9, "float32": 10, "float64": 11}
+
+
+def ingest_frames(src, row_major: bool = False, stream: int = 0):
+    """Camera frames (device tensor (n_frames, a, b) of any supported dtype;
+    column-major frames are (n_frames, n_cols, n_rows), row-major ones
+    (n_frames, n_rows, n_cols)) -> (uint16 stack as int16 tensor (n_frames,
+    n_cols, n_rows), number of pixels rounded or clamped)."""
+    import torch
+    name = str(src.dtype).replace("torch.", "")
+    if name not in STORAGE_FORMATS:
+        raise LocalizerError(f"unsupported frame dtype {src.dtype}")
+    src = src.contiguous()
+    n_frames = src.shape[0]
+    n_rows, n_cols = (src.shape[1], src.shape[2]) if row_major else (src.shape[2], src.shape[1])
+    out = torch.empty((n_frames, n_cols, n_rows), dtype=torch.int16, device=src.device)
+    lossy = _check(lib().loc_ingest_frames(C.c_void_p(src.data_ptr()), STORAGE_FORMATS[name], n_frames, n_rows,
+                                           n_cols, int(row_major), C.c_void_p(out.data_ptr()), C.c_void_p(stream)))
+    return out, lossy
 
 
 def write_positions(path: str, rows: np.ndarray, flags: np.ndarray | None, method: int, header: str = "") -> int:

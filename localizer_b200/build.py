@@ -22,7 +22,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
                   "-I" + os.path.join(ROOT, "include")]
-SOURCES = ["loc_fit.cu", "loc_capi.cu", "loc_finder.cpp", "loc_synth.cu", "loc_static.cu", "loc_proposal.cu", "loc_finder_gpu.cu", "loc_writer.cpp"]
+SOURCES = ["loc_fit.cu", "loc_capi.cu", "loc_finder.cpp", "loc_synth.cu", "loc_static.cu", "loc_proposal.cu", "loc_finder_gpu.cu", "loc_writer.cpp", "loc_ingest.cu"]
 
 
 def _headers():

@@ -1,0 +1,135 @@
+// Frame ingest: camera buffers of any of the reference's storage types
+// (LocalizerStorageType, reference source/Defines.h:82-95) in row- or
+// column-major order (BufferWithFormatToImage / CopyBufferToImage,
+// source/FileIO.cpp:195-234, FileIO.h:96-116) into the fit path's uint16
+// frame stack (x fastest). The reference widens every pixel to double; the
+// fit path works on uint16, which holds every value of 8- and 16-bit unsigned
+// cameras exactly. Other values are rounded to the nearest integer and
+// clamped to [0, 65535]; the call returns how many pixels that changed, so a
+// caller can tell a lossless ingest (0) from a lossy one.
+//
+// Column-major input is a streaming conversion; row-major input is
+// transposed through 32 x 32 shared-memory tiles so that both the reads and
+// the writes are coalesced. HBM-bound: element size + 2 bytes per pixel.
+#include "../../include/localizer_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <string>
+#include <type_traits>
+
+namespace locb {
+int record_error_fixed(int code, const char *msg);
+}
+
+namespace {
+
+constexpr int kTile = 32;
+
+template <typename S> __device__ __forceinline__ uint16_t to_u16(S v, unsigned &lossy)
+{
+    if constexpr (sizeof(S) <= 2 && !std::is_signed<S>::value) {
+        return (uint16_t)v;
+    } else {
+        const double d = (double)v;
+        double r = rint(d);
+        r = r < 0.0 ? 0.0 : (r > 65535.0 ? 65535.0 : r);
+        if (!(r == d)) ++lossy;   // rounded, clamped, or NaN (-> 0)
+        return (uint16_t)(r == r ? r : 0.0);
+    }
+}
+
+__device__ __forceinline__ void count_lossy(unsigned lossy, unsigned long long *counter)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lossy += __shfl_xor_sync(0xffffffffu, lossy, o);
+    if ((threadIdx.x & 31) == 0 && lossy) atomicAdd(counter, (unsigned long long)lossy);
+}
+
+// column-major: the same pixel order on both sides
+template <typename S>
+__global__ void k_ingest_cm(const S *src, uint16_t *dst, long long n, unsigned long long *lossy_count)
+{
+    unsigned lossy = 0;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        dst[p] = to_u16<S>(src[p], lossy);
+    count_lossy(lossy, lossy_count);
+}
+
+// row-major: frame buffer element (i, j) at i * n_cols + j -> pixel i + j * n_rows
+template <typename S>
+__global__ void k_ingest_rm(const S *src, uint16_t *dst, int n_rows, int n_cols, unsigned long long *lossy_count)
+{
+    __shared__ uint16_t t[kTile][kTile + 1];
+    const int f = blockIdx.z;
+    const size_t fpx = (size_t)n_rows * n_cols;
+    const int j0 = blockIdx.x * kTile, i0 = blockIdx.y * kTile;   // tile: rows i (image rows), cols j
+    unsigned lossy = 0;
+    // read: consecutive threads along j (contiguous in the row-major buffer)
+    for (int di = threadIdx.y; di < kTile; di += blockDim.y) {
+        const int i = i0 + di, j = j0 + threadIdx.x;
+        if (i < n_rows && j < n_cols) t[di][threadIdx.x] = to_u16<S>(src[f * fpx + (size_t)i * n_cols + j], lossy);
+    }
+    __syncthreads();
+    // write: consecutive threads along i (contiguous in the column-major stack)
+    for (int dj = threadIdx.y; dj < kTile; dj += blockDim.y) {
+        const int i = i0 + threadIdx.x, j = j0 + dj;
+        if (i < n_rows && j < n_cols) dst[f * fpx + i + (size_t)j * n_rows] = t[threadIdx.x][dj];
+    }
+    count_lossy(lossy, lossy_count);
+}
+
+template <typename S>
+cudaError_t launch(const void *src, uint16_t *dst, int n_frames, int n_rows, int n_cols, int row_major,
+                   unsigned long long *cnt, cudaStream_t st)
+{
+    const S *s = static_cast<const S *>(src);
+    if (!row_major) {
+        const long long n = (long long)n_frames * n_rows * n_cols;
+        const int blocks = (int)((n + 255) / 256 < 148 * 32 ? (n + 255) / 256 : 148 * 32);
+        k_ingest_cm<S><<<blocks, 256, 0, st>>>(s, dst, n, cnt);
+    } else {
+        dim3 grid((n_cols + kTile - 1) / kTile, (n_rows + kTile - 1) / kTile, n_frames);
+        k_ingest_rm<S><<<grid, dim3(kTile, 8), 0, st>>>(s, dst, n_rows, n_cols, cnt);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" LOC_API long long loc_ingest_frames(const void *d_src, int format, int n_frames, int n_rows, int n_cols,
+                                               int row_major, uint16_t *d_dst, void *stream)
+{
+    if (!d_src || !d_dst || n_frames < 0 || n_rows <= 0 || n_cols <= 0)
+        return locb::record_error_fixed(LOC_E_INVALID, "bad argument");
+    if (n_frames > 65535 && row_major) return locb::record_error_fixed(LOC_E_UNSUPPORTED, "too many frames in one call");
+    if (n_frames == 0) return 0;
+    const cudaStream_t st = (cudaStream_t)stream;
+    unsigned long long *cnt = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&cnt, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return locb::record_error_fixed(LOC_E_NOMEM, "ingest counter");
+    cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st);
+    switch (format) {
+    case 2: e = launch<int8_t>(d_src, d_dst, n_frames, n_rows, n_cols, row_major, cnt, st); break;
+    case 3: e = launch<uint8_t>(d_src, d_dst, n_frames, n_rows, n_cols, row_major, cnt, st); break;
+    case 4: e = launch<int16_t>(d_src, d_dst, n_frames, n_rows, n_cols, row_major, cnt, st); break;
+    case 5: e = launch<uint16_t>(d_src, d_dst, n_frames, n_rows, n_cols, row_major, cnt, st); break;
+    case 6: e = launch<int32_t>(d_src, d_dst, n_frames, n_rows, n_cols, row_major, cnt, st); break;
+    case 7: e = launch<uint32_t>(d_src, d_dst, n_frames, n_rows, n_cols, row_major, cnt, st); break;
+    case 8: e = launch<int64_t>(d_src, d_dst, n_frames, n_rows, n_cols, row_major, cnt, st); break;
+    case 9: e = launch<uint64_t>(d_src, d_dst, n_frames, n_rows, n_cols, row_major, cnt, st); break;
+    case 10: e = launch<float>(d_src, d_dst, n_frames, n_rows, n_cols, row_major, cnt, st); break;
+    case 11: e = launch<double>(d_src, d_dst, n_frames, n_rows, n_cols, row_major, cnt, st); break;
+    default:
+        cudaFreeAsync(cnt, st);
+        return locb::record_error_fixed(LOC_E_UNSUPPORTED, "unsupported storage format (4-bit types are not)");
+    }
+    unsigned long long h = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, cnt, sizeof h, cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(cnt, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return locb::record_error_fixed(LOC_E_CUDA, (std::string("ingest: ") + cudaGetErrorString(e)).c_str());
+    return (long long)h;
+}
