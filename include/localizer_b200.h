@@ -34,6 +34,12 @@ extern "C" {
 #define LOC_METHOD_2DGAUSS 0                          /* FitPositions_SymmetricGaussian */
 #define LOC_METHOD_2DGAUSS_FIXEDWIDTH 1               /* FitPositions_FixedWidthGaussian */
 #define LOC_METHOD_2DGAUSS_ELLIPSOIDAL 5              /* FitPositions_EllipsoidalGaussian_SymmetricPSF */
+#define LOC_METHOD_MLEWG 6                            /* FitPositions_MLEwG: FP64 Nelder-Mead maximum
+                                                         likelihood (Localization.cpp:633-789); output
+                                                         columns frame, integral, width, x, y,
+                                                         background, position deviation, frames
+                                                         present; sigma is unused; not available in
+                                                         loc_fit_batch_static or with a proposal */
 #define LOC_METHOD_2DGAUSS_ELLIPSOIDAL_ASTIGMATISM 7  /* FitPositions_EllipsoidalGaussian */
 
 /* Per-candidate reject codes (0 = kept: the candidate produced an output row
@@ -49,6 +55,7 @@ extern "C" {
 #define LOC_FLAG_SYMPSF_RATIO 8    /* method 5: axis ratio outside [0.75, 1.25], :616 */
 #define LOC_FLAG_SYMPSF_WIDTH 9    /* method 5: no axis in [0.7, 1.3] w0, :621 */
 #define LOC_FLAG_BAD_INPUT 10      /* frame index out of range or non-finite candidate */
+#define LOC_FLAG_INTEGRAL 11       /* MLEwG: integral outside [1/2, 3/2] of the start, :753 */
 
 /* Termination status column (the value of the reference's solver loop at
  * exit, Localization.cpp:148-155): 0 converged (test_delta), 1 iteration

@@ -20,12 +20,13 @@ LIB_PATH = os.path.join(HERE, "liblocalizer_b200.so")
 METHOD_2DGAUSS = 0
 METHOD_2DGAUSS_FIXEDWIDTH = 1
 METHOD_2DGAUSS_ELLIPSOIDAL = 5
+METHOD_MLEWG = 6
 METHOD_2DGAUSS_ELLIPSOIDAL_ASTIGMATISM = 7
 
 FLAGS = {0: "kept", 1: "edge", 2: "amplitude", 3: "out_of_window", 4: "width_range", 5: "drift",
          6: "eigen", 7: "no_axis", 8: "sympsf_ratio", 9: "sympsf_width", 10: "bad_input"}
 
-REF_COLUMNS = {0: 12, 1: 10, 5: 16, 7: 16}
+REF_COLUMNS = {0: 12, 1: 10, 5: 16, 6: 8, 7: 16}
 N_PARAMS = {0: 5, 1: 4, 5: 7, 7: 7}
 
 COLUMN_NAMES = {
@@ -37,6 +38,7 @@ COLUMN_NAMES = {
         "sigma2_dev", "x_dev", "y_dev", "theta_dev", "background_dev", "n_frames"],
 }
 COLUMN_NAMES[5] = COLUMN_NAMES[7]
+COLUMN_NAMES[6] = ["frame", "integral", "width", "x", "y", "background", "position_dev", "n_frames"]
 
 CANDIDATE_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("intensity", "<f8"), ("background", "<f8"),
                             ("frame", "<i4"), ("half_width", "<i4")], align=True)
@@ -376,6 +378,15 @@ class FitPositions_EllipsoidalGaussian(FitPositions):
 
 class FitPositions_EllipsoidalGaussian_SymmetricPSF(FitPositions):
     method = METHOD_2DGAUSS_ELLIPSOIDAL
+
+
+class FitPositions_MLEwG(FitPositions):
+    """Maximum-likelihood fit with a Gaussian (reference FitPositions_MLEwG,
+    Localization.h:126-136): takes the PSF width only."""
+    method = METHOD_MLEWG
+
+    def __init__(self, initialPSFWidth: float, half_width: int = 0, engine: Engine | None = None):
+        super().__init__(initialPSFWidth, 1.0, half_width, engine)
 
 
 def LocalizerFitEmitters(image_data: np.ndarray, psf_width: float, glrt_insensitivity: float) -> np.ndarray:

@@ -22,7 +22,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
                   "-I" + os.path.join(ROOT, "include")]
-SOURCES = ["loc_fit.cu", "loc_capi.cu", "loc_finder.cpp", "loc_synth.cu", "loc_static.cu", "loc_proposal.cu", "loc_finder_gpu.cu", "loc_writer.cpp", "loc_ingest.cu"]
+SOURCES = ["loc_fit.cu", "loc_capi.cu", "loc_finder.cpp", "loc_synth.cu", "loc_static.cu", "loc_proposal.cu", "loc_finder_gpu.cu", "loc_writer.cpp", "loc_ingest.cu", "loc_mlewg.cu"]
 
 
 def _headers():
@@ -44,6 +44,9 @@ def _compile(src, verbose=False):
     if not _stale(obj, deps):
         return obj
     cmd = [NVCC] + NVFLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
+    if src == "loc_mlewg.cu":
+        # the MLEwG fits follow the reference's FP64 operation order: no contraction into FMA
+        cmd.insert(1, "--fmad=false")
     if src.endswith(".cpp"):
         cmd = [NVCC, "-x", "cu"] + NVFLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
     if verbose:

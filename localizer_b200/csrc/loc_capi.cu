@@ -32,7 +32,7 @@ int cuda_fail(cudaError_t e, const char *where)
     return fail(LOC_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
-int method_ok(int m) { return m == 0 || m == 1 || m == 5 || m == 7; }
+int method_ok(int m) { return m == 0 || m == 1 || m == 5 || m == 6 || m == 7; }
 
 // Device buffer that grows on demand.
 struct DevBuf {
@@ -97,7 +97,7 @@ LOC_API void loc_default_options(loc_options *opt)
 LOC_API int loc_reference_columns(int method)
 {
     if (!method_ok(method)) return fail(LOC_E_UNSUPPORTED, "unsupported method code");
-    return method == 0 ? 12 : method == 1 ? 10 : 16;
+    return method == 0 ? 12 : method == 1 ? 10 : method == 6 ? 8 : 16;
 }
 
 LOC_API int loc_output_columns(int method)
@@ -109,7 +109,7 @@ LOC_API int loc_output_columns(int method)
 LOC_API int loc_parameter_count(int method)
 {
     if (!method_ok(method)) return fail(LOC_E_UNSUPPORTED, "unsupported method code");
-    return method == 0 ? 5 : method == 1 ? 4 : 7;
+    return method == 0 || method == 6 ? 5 : method == 1 ? 4 : 7;
 }
 
 LOC_API int loc_ctx_create(loc_ctx **ctx, int device)

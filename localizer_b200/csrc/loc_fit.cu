@@ -1176,6 +1176,11 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
     if (rerun && (e = cudaMemsetAsync(s.meta2, 0, sizeof(int) * kMetaInts, stream)) != cudaSuccess) return e;
     e = cudaMemsetAsync(s.stats, 0, sizeof(unsigned long long) * kStatWords, stream);
     if (e != cudaSuccess) return e;
+    if (p.method == 6) {
+        for (int k = 0; k < 4; ++k)
+            if (p.ev[k]) cudaEventRecord(p.ev[k], stream);
+        return enqueue_mlewg(p, s.stats, stream);
+    }
     if (n == 0) {
         for (int k = 0; k < 4; ++k)
             if (p.ev[k]) cudaEventRecord(p.ev[k], stream);

@@ -76,4 +76,7 @@ constexpr int kStatWords = 2 * 12 + 2;  // solver counters, FP64 re-run counters
 // *used_smem_side receives the ROI side the solver was sized for.
 cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t stream, int *err_detail);
 
+// MLEwG (method 6): one kernel, no scratch but the statistics counters.
+cudaError_t enqueue_mlewg(const FitParams &p, unsigned long long *stats, cudaStream_t stream);
+
 }  // namespace locb

@@ -1,7 +1,7 @@
 // Localized-positions text writer in the reference's format
 // (LocalizedPositionsContainer_*::writePositionsToFile, reference
 // source/Storage.cpp:292-345 symmetric, 427-470 fixed width, 642-700
-// ellipsoidal): a title line naming the fit, the caller's header line,
+// ellipsoidal, 1128-1175 MLEwG): a title line naming the fit, the caller's header line,
 // "DATA FOLLOWS", the column titles, then one tab-separated line per kept
 // position. Frame numbers and the frames-present count are integers; every
 // other value is written as a default-formatted C++ stream writes a double
@@ -24,10 +24,11 @@ int record_error_fixed(int code, const char *msg);
 
 namespace {
 
-const char *const kTitle[3] = {
+const char *const kTitle[4] = {
     "Localized positions using symmetric 2D Gauss fitting",
     "Localized positions using symmetric 2D Gauss fitting with fixed PSF width",
     "Localized positions using ellipsoidal 2D Gauss fitting",
+    "Localized positions using MLEwG estimation",
 };
 
 const char *const kCols0[] = {"First frame", "Integrated intensity", "Fitted PSF standard deviation (pixel)",
@@ -47,6 +48,10 @@ const char *const kCols7[] = {"First frame", "Integrated intensity",
                               "PSF width deviation along second principal axis (pixel)",
                               "X position deviation (pixel)", "Y position deviation (pixel)", "Rotation deviation",
                               "Background deviation", "Number of frames where this emitter is present"};
+
+const char *const kCols6[] = {"First frame", "Integrated intensity", "Fitted PSF standard deviation (pixel)",
+                              "X position (pixel)", "Y position (pixel)", "Background", "Position deviation (pixel)",
+                              "Number of frames where this emitter is present"};
 
 void format_row(std::string &s, const double *row, int ncol)
 {
@@ -69,11 +74,11 @@ extern "C" LOC_API long loc_write_positions_text(const double *rows, const uint8
 {
     if (!path || n < 0 || (n > 0 && !rows))
         return locb::record_error_fixed(LOC_E_INVALID, "bad argument");
-    if (!(method == 0 || method == 1 || method == 5 || method == 7))
+    if (!(method == 0 || method == 1 || method == 5 || method == 6 || method == 7))
         return locb::record_error_fixed(LOC_E_UNSUPPORTED, "unsupported method code");
-    const int ref_cols = method == 0 ? 12 : method == 1 ? 10 : 16;
+    const int ref_cols = method == 0 ? 12 : method == 1 ? 10 : method == 6 ? 8 : 16;
     const int stride = ref_cols + 2;  // rows as the fit calls write them
-    const char *const *cols = method == 0 ? kCols0 : method == 1 ? kCols1 : kCols7;
+    const char *const *cols = method == 0 ? kCols0 : method == 1 ? kCols1 : method == 6 ? kCols6 : kCols7;
     std::vector<long> kept;
     kept.reserve((size_t)n);
     for (long i = 0; i < n; ++i)
@@ -83,7 +88,7 @@ extern "C" LOC_API long loc_write_positions_text(const double *rows, const uint8
     FILE *f = std::fopen(path, "wb");
     if (!f) return locb::record_error_fixed(LOC_E_INVALID, "Unable to create the output file");
     std::string head;
-    head += kTitle[method == 0 ? 0 : method == 1 ? 1 : 2];
+    head += kTitle[method == 0 ? 0 : method == 1 ? 1 : method == 6 ? 3 : 2];
     head += "\n";
     head += header ? header : "";
     head += "\nDATA FOLLOWS\n";

@@ -5,10 +5,10 @@
  * 1.16 headers vendored in the reference (include/gsl) for the struct
  * layouts only; it implements just the GSL entry points those three files
  * import (gsl_vector/gsl_matrix allocation, gsl_blas_dnrm2, the lmsder
- * fdfsolver, gsl_multifit_test_delta, gsl_multifit_covar). The Nelder-Mead
- * and lngamma entry points of the MLEwG fitter (Localization.cpp:633-789,
- * not a Gaussian LM fitter) are present only so the library links; they
- * report failure if called.
+ * fdfsolver, gsl_multifit_test_delta, gsl_multifit_covar) and, for the MLEwG
+ * fitter (Localization.cpp:633-789), the nmsimplex2 minimiser over the
+ * restatement in nmsimplex_core.c, gsl_multimin_test_size and
+ * gsl_sf_lngamma (log |Gamma|, from libm).
  *
  * It also records, per solver set() call, how many iterate() calls followed
  * and the last status, so the harness can read the reference's iteration
@@ -26,6 +26,8 @@
 #include <string.h>
 
 #include "lmsder_core.h"
+#include "nmsimplex_core.h"
+#include <math.h>
 
 gsl_vector *gsl_vector_alloc(const size_t n)
 {
@@ -246,45 +248,116 @@ int gsl_multifit_covar(const gsl_matrix *J, double epsrel, gsl_matrix *covar)
     return GSL_SUCCESS;
 }
 
-/* ---- not on the Gaussian LM path: report failure ---- */
+/* ---- Nelder-Mead minimiser (MLEwG fitter, Localization.cpp:633-789) ---- */
 
-const gsl_multimin_fminimizer_type *gsl_multimin_fminimizer_nmsimplex2 = NULL;
+typedef struct {
+    nm_state nm;
+    gsl_multimin_function *fn;
+    size_t n;
+} nm_shim_state;
+
+static double nm_tramp(const double *x, void *par)
+{
+    nm_shim_state *s = (nm_shim_state *)par;
+    gsl_vector xv = {s->n, 1, (double *)x, NULL, 0};
+    return GSL_MULTIMIN_FN_EVAL(s->fn, &xv);
+}
+
+static int nms_alloc(void *vstate, size_t n)
+{
+    nm_shim_state *s = (nm_shim_state *)vstate;
+    if (n < 1 || n > NM_NMAX) return GSL_EINVAL;
+    s->n = n;
+    return GSL_SUCCESS;
+}
+
+static int nms_set(void *vstate, gsl_multimin_function *f, const gsl_vector *x, double *size,
+                   const gsl_vector *step_size)
+{
+    nm_shim_state *s = (nm_shim_state *)vstate;
+    double xa[NM_NMAX], st[NM_NMAX];
+    for (size_t i = 0; i < s->n; i++) {
+        xa[i] = x->data[i * x->stride];
+        st[i] = step_size->data[i * step_size->stride];
+    }
+    s->fn = f;
+    if (g_log_iters && g_log_n < LOG_CAP) {
+        g_log_iters[g_log_n] = 0;
+        g_log_status[g_log_n] = 0;
+        g_log_n++;
+    }
+    return nm_set(&s->nm, (int)s->n, nm_tramp, s, xa, st, size);
+}
+
+static int nms_iterate(void *vstate, gsl_multimin_function *f, gsl_vector *x, double *size, double *fval)
+{
+    nm_shim_state *s = (nm_shim_state *)vstate;
+    double xa[NM_NMAX];
+    s->fn = f;
+    const int rc = nm_iterate(&s->nm, nm_tramp, s, xa, size, fval);
+    if (rc == 0)
+        for (size_t i = 0; i < s->n; i++) x->data[i * x->stride] = xa[i];
+    if (g_log_iters && g_log_n > 0) {
+        g_log_iters[g_log_n - 1]++;
+        g_log_status[g_log_n - 1] = rc;
+    }
+    return rc;
+}
+
+static void nms_free(void *vstate) { (void)vstate; }
+
+static const gsl_multimin_fminimizer_type nmsimplex2_type = {
+    "nmsimplex2", sizeof(nm_shim_state), nms_alloc, nms_set, nms_iterate, nms_free};
+
+const gsl_multimin_fminimizer_type *gsl_multimin_fminimizer_nmsimplex2 = &nmsimplex2_type;
 
 gsl_multimin_fminimizer *gsl_multimin_fminimizer_alloc(const gsl_multimin_fminimizer_type *T, size_t n)
 {
-    (void)T; (void)n;
-    return NULL;
+    if (!T) return NULL;
+    gsl_multimin_fminimizer *s = (gsl_multimin_fminimizer *)calloc(1, sizeof(*s));
+    if (!s) return NULL;
+    s->state = calloc(1, T->size);
+    s->x = gsl_vector_alloc(n);
+    if (!s->state || !s->x || T->alloc(s->state, n) != GSL_SUCCESS) {
+        gsl_vector_free(s->x);
+        free(s->state);
+        free(s);
+        return NULL;
+    }
+    s->type = T;
+    return s;
 }
 
-void gsl_multimin_fminimizer_free(gsl_multimin_fminimizer *s) { (void)s; }
-
-int gsl_multimin_fminimizer_set(gsl_multimin_fminimizer *s, gsl_multimin_function *f,
-                                const gsl_vector *x, const gsl_vector *step_size)
+void gsl_multimin_fminimizer_free(gsl_multimin_fminimizer *s)
 {
-    (void)s; (void)f; (void)x; (void)step_size;
-    return GSL_FAILURE;
+    if (!s) return;
+    s->type->free(s->state);
+    free(s->state);
+    gsl_vector_free(s->x);
+    free(s);
+}
+
+int gsl_multimin_fminimizer_set(gsl_multimin_fminimizer *s, gsl_multimin_function *f, const gsl_vector *x,
+                                const gsl_vector *step_size)
+{
+    if (s->x->size != f->n || x->size != f->n || step_size->size != f->n) return GSL_EBADLEN;
+    s->f = f;
+    for (size_t i = 0; i < x->size; i++) s->x->data[i] = x->data[i * x->stride];
+    return s->type->set(s->state, f, x, &s->size, step_size);
 }
 
 int gsl_multimin_fminimizer_iterate(gsl_multimin_fminimizer *s)
 {
-    (void)s;
-    return GSL_FAILURE;
+    return s->type->iterate(s->state, s->f, s->x, &s->size, &s->fval);
 }
 
-double gsl_multimin_fminimizer_size(const gsl_multimin_fminimizer *s)
-{
-    (void)s;
-    return 0.0;
-}
+double gsl_multimin_fminimizer_size(const gsl_multimin_fminimizer *s) { return s->size; }
 
 int gsl_multimin_test_size(const double size, double epsabs)
 {
-    (void)size; (void)epsabs;
-    return GSL_FAILURE;
+    if (epsabs < 0.0) return GSL_EBADTOL;
+    return size < epsabs ? GSL_SUCCESS : GSL_CONTINUE;
 }
 
-double gsl_sf_lngamma(const double x)
-{
-    (void)x;
-    return 0.0;
-}
+/* log |Gamma(x)| (the reference only calls it at integer + 1) */
+double gsl_sf_lngamma(const double x) { return lgamma(x); }

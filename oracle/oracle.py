@@ -24,8 +24,8 @@ CAND_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("intensity", "<f8"), ("backg
                        ("frame", "<i4"), ("half_width", "<i4")], align=True)
 assert CAND_DTYPE.itemsize == 40
 
-REF_COLUMNS = {0: 12, 1: 10, 5: 16, 7: 16}
-N_PARAMS = {0: 5, 1: 4, 5: 7, 7: 7}
+REF_COLUMNS = {0: 12, 1: 10, 5: 16, 6: 8, 7: 16}
+N_PARAMS = {0: 5, 1: 4, 5: 7, 6: 5, 7: 7}
 
 
 class _Options(C.Structure):

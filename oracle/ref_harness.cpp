@@ -80,13 +80,18 @@ std::shared_ptr<FitPositions> make_fitter(int method, double w0, double sigma, s
         f->ellipsoidalFitter.cutoff_radius = r;
         return f;
     }
+    case 6: {
+        auto f = std::make_shared<FitPositions_MLEwG>(w0);   /* no noise weight */
+        f->cutoff_radius = r;
+        return f;
+    }
     }
     return nullptr;
 }
 
 int ref_cols(int method)
 {
-    return method == 0 ? 12 : method == 1 ? 10 : 16;
+    return method == 0 ? 12 : method == 1 ? 10 : method == 6 ? 8 : 16;
 }
 
 } // namespace

@@ -6,7 +6,8 @@ lmsder restatement) on small seeded synthetic stacks and stores frames,
 candidates and the reference's output matrices, kept flags and iteration
 counts. Needs the reference tree, so it runs only where it exists:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # all fixtures
+    python tests/golden/make_golden.py mlewg      # mlewg.npz only
 """
 from __future__ import annotations
 
@@ -68,5 +69,26 @@ def main():
         np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **payload)
 
 
+def main_mlewg():
+    """mlewg.npz: the reference's MLEwG fitter (FitPositions_MLEwG, method 6)
+    on the small workload's frames and candidates (the Nelder-Mead minimiser
+    it calls is the restatement in oracle/nmsimplex_core.c)."""
+    if not O.ref_available():
+        O.build()
+    w = synth.scaled(synth.workloads()["small"], 4)
+    frames, _ = synth.make(w)
+    cands = O.candidates(frames, 30.0, 1.3, half_widths=w.half_widths, seed=w.seed, use_ref=True)
+    cands = np.concatenate([cands, edge_candidates(frames, 1.3, 4)])
+    out, kept, iters, status = O.ref_fit(frames, cands, 6, 1.3)
+    print(f"mlewg: {len(cands)} candidates, {kept.sum()} kept, mean iterations {iters[iters >= 0].mean():.1f}")
+    np.savez_compressed(os.path.join(OUT, "mlewg.npz"), frames=frames,
+                        cands=cands.view(np.uint8).reshape(len(cands), -1), w0=1.3, pfa=30.0,
+                        methods=np.array([6]), out_6=out, kept_6=kept, iters_6=iters, status_6=status)
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "mlewg":
+        main_mlewg()
+    else:
+        main()
+        main_mlewg()

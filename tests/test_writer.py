@@ -23,7 +23,8 @@ def _frame_group(g):
 
 
 @pytest.mark.skipif(not O.ref_available(), reason="reference build absent")
-@pytest.mark.parametrize("name,method", [("small", 0), ("small", 1), ("uneven", 7), ("uneven", 5), ("stress", 0)])
+@pytest.mark.parametrize("name,method", [("small", 0), ("small", 1), ("uneven", 7), ("uneven", 5), ("stress", 0),
+                                         ("mlewg", 6)])
 def test_text_file_matches_reference_writer(name, method):
     g = G.load(name)
     frames = g["frames"]
