@@ -176,6 +176,9 @@ __device__ int nm_iterate(Simplex &s, const Roi &roi, double *x, double &size)
             compute_size(s);
             if (bad) return 5;
         }
+    } else {
+        // better than the second-worst corner: replace the worst by the reflection
+        update_point(s, hi, xc, val);
     }
     lo = 0;
     for (int i = 1; i < NP; i++)
