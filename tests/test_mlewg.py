@@ -17,7 +17,7 @@ from oracle import oracle as O
 from tests import _golden as G
 
 POS_TOL = 1e-3
-FRACTION = 0.98
+FRACTION = 0.995   # measured: every fit identical to the reference on both sets
 
 
 def _compare(rows, flags, ref, kept):
