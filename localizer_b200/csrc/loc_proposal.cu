@@ -61,14 +61,16 @@ namespace locb {
 namespace {
 
 constexpr int kWin = 11, kWin2 = 121;
-constexpr int kR = 16;                            // windows per CTA iteration
+constexpr int kR = 8;                             // windows per CTA iteration
 constexpr int kRows = 81 * kR;                    // activation grid rows per iteration
 constexpr int kTiles = (kRows + 127) / 128;       // M = 128 tiles
 constexpr int kRowsAlloc = kTiles * 128 + 24;     // + largest tap shift (20), multiple of 8
 constexpr uint32_t kLBO = kRowsAlloc * 16;        // bytes between 8-channel chunks
-constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kTmemCols = 256;
 static_assert(kTiles * 32 <= (int)kTmemCols, "accumulators must fit in tensor memory");
-constexpr int kThreads = 256;
+constexpr int kThreads = 128;               // 4 warps: one TMEM lane quarter each
+constexpr int kCtasPerSm = 2;               // two CTAs per SM overlap tensor and CUDA-core phases
+constexpr int kBwdThreads = 256;            // backward pass block (its conv1 step uses 160 threads)
 constexpr float kSigmaRef = 1.5f;
 constexpr int kWaitLimit = 1 << 20;
 
@@ -94,13 +96,12 @@ constexpr int SO_WP = SO_ACT2 + 4 * (int)kLBO;
 constexpr int SO_V = SO_WP + kWP * 2;
 constexpr int SO_W1 = SO_V + kR * kWin2 * 4;      // w1 + b1
 constexpr int SO_B23 = SO_W1 + 160 * 4;           // b2 + b3
-constexpr int SO_WH = SO_B23 + 64 * 4;            // head weights + bias (up to 8 outputs)
-constexpr int SO_HACC = SO_WH + 8 * 801 * 4;
+constexpr int SO_HACC = SO_B23 + 64 * 4;          // head outputs (head weights are read through L1)
 constexpr int SO_STAT = SO_HACC + kR * 8 * 4;
 constexpr int SO_BAR = SO_STAT + kR * 4 * 4;
 constexpr int SO_MISC = SO_BAR + 8;
 constexpr int kSmemFwd = SO_MISC + 16;
-static_assert(kSmemFwd <= 227 * 1024, "forward kernel shared memory");
+static_assert(kCtasPerSm * (kSmemFwd + 1024) <= 228 * 1024, "two forward CTAs per SM");
 static_assert(SO_ACT2 % 16 == 0 && SO_WP % 16 == 0 && SO_V % 16 == 0 && SO_BAR % 8 == 0, "alignment");
 
 constexpr uint32_t kIdesc = tc::idesc_bf16_f32<128, 32>();
@@ -197,7 +198,7 @@ struct FwdArgs {
 };
 
 template <int NOUT, int MODE>
-__global__ void __launch_bounds__(kThreads, 1) k_prop_fwd(FwdArgs a)
+__global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -207,7 +208,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_prop_fwd(FwdArgs a)
     float *v = reinterpret_cast<float *>(sm + SO_V);
     float *w1 = reinterpret_cast<float *>(sm + SO_W1);
     float *b23 = reinterpret_cast<float *>(sm + SO_B23);
-    float *wh = reinterpret_cast<float *>(sm + SO_WH);
+    const float *wh = a.w + kWH;
     float *hacc = reinterpret_cast<float *>(sm + SO_HACC);
     float *stat = reinterpret_cast<float *>(sm + SO_STAT);
 
@@ -221,7 +222,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_prop_fwd(FwdArgs a)
             b23[k] = a.w[kB2 + k];
             b23[32 + k] = a.w[kB3 + k];
         }
-        for (int k = tid; k < NOUT * 801; k += kThreads) wh[k] = a.w[kWH + k];
         for (int k = tid; k < kR * 8; k += kThreads) hacc[k] = 0.f;
         // padding rows past the last window: read only by discarded outputs,
         // zeroed so that they hold finite values
@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_prop_fwd(FwdArgs a)
     const uint32_t tmem = *tslot;
     uint32_t phase = 0;
     bool failed = false;
-    const int q = warp & 3, h = warp >> 2;   // epilogue: TMEM lane quarter, column half
+    const int q = warp;   // epilogue: the warp's TMEM lane quarter (4 warps)
     const uint32_t t_lane = (uint32_t)(32 * q) << 16;
     const float *bh = wh + NOUT * 800;
 
@@ -383,7 +383,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_prop_fwd(FwdArgs a)
         }
         tc::fence_after_sync();
         // ---- 5. conv2 epilogue: bias, ReLU, BF16 -> act2 ----
-        for (int i = 0; i < kTiles; ++i) {
+        for (int i = 0; i < kTiles; ++i)
+        for (int h = 0; h < 2; ++h) {
             float acc[16];
             tc::tmem_ld16(tmem + t_lane + (uint32_t)(i * 32 + 16 * h), acc);
             tc::tmem_ld_wait();
@@ -441,7 +442,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_prop_fwd(FwdArgs a)
         // ---- 7. conv3 epilogue: bias, ReLU -> a3 in shared memory (the
         // activation buffers are free once the conv3 MMAs have completed) ----
         float *a3s = reinterpret_cast<float *>(sm + SO_ACT2);   // [kR][kA3Stride], (channel, position)
-        for (int i = 0; i < kTiles; ++i) {
+        for (int i = 0; i < kTiles; ++i)
+        for (int h = 0; h < 2; ++h) {
             float acc[16];
             tc::tmem_ld16(tmem + t_lane + (uint32_t)(i * 32 + 16 * h), acc);
             tc::tmem_ld_wait();
@@ -620,7 +622,7 @@ template <int NOUT> struct BwdSmem {
 };
 
 template <int NOUT>
-__global__ void __launch_bounds__(kThreads, 1) k_prop_bwd(BwdArgs a)
+__global__ void __launch_bounds__(kBwdThreads, 1) k_prop_bwd(BwdArgs a)
 {
     using L = BwdSmem<NOUT>;
     extern __shared__ __align__(16) float bs[];
@@ -629,25 +631,25 @@ __global__ void __launch_bounds__(kThreads, 1) k_prop_bwd(BwdArgs a)
     float *w2 = bs + L::W2, *w3 = bs + L::W3;
     float *v = bs + L::V, *a1 = bs + L::A1, *a2 = bs + L::A2, *z3 = bs + L::Z3, *z2 = bs + L::Z2, *z1 = bs + L::Z1;
     float *dO = bs + L::DO;
-    for (int k = tid; k < L::NW; k += kThreads) g[k] = 0.f;
-    for (int k = tid; k < 4608; k += kThreads) w2[k] = __bfloat162float(__float2bfloat16_rn(a.w[kW2 + k]));
-    for (int k = tid; k < 9216; k += kThreads) w3[k] = __bfloat162float(__float2bfloat16_rn(a.w[kW3 + k]));
+    for (int k = tid; k < L::NW; k += kBwdThreads) g[k] = 0.f;
+    for (int k = tid; k < 4608; k += kBwdThreads) w2[k] = __bfloat162float(__float2bfloat16_rn(a.w[kW2 + k]));
+    for (int k = tid; k < 9216; k += kBwdThreads) w3[k] = __bfloat162float(__float2bfloat16_rn(a.w[kW3 + k]));
     const float *wh = a.w + kWH;
     float lsum = 0.f;
     __syncthreads();
     for (int b = blockIdx.x; b < a.n; b += gridDim.x) {
         // ---- load this window's activations ----
-        for (int k = tid; k < kWin2; k += kThreads) v[k] = a.save_v[(size_t)b * kWin2 + k];
-        for (int k = tid; k < 81 * 16; k += kThreads) {
+        for (int k = tid; k < kWin2; k += kBwdThreads) v[k] = a.save_v[(size_t)b * kWin2 + k];
+        for (int k = tid; k < 81 * 16; k += kBwdThreads) {
             const int p = k >> 4, c = k & 15;
             a1[c * 81 + p] = __bfloat162float(a.save_a1[(size_t)b * 81 * 16 + k]);
         }
-        for (int k = tid; k < 49 * 32; k += kThreads) {
+        for (int k = tid; k < 49 * 32; k += kBwdThreads) {
             const int p49 = k >> 5, c = k & 31;
             const int pos = (p49 / 7) * 9 + p49 % 7;
             a2[c * 49 + p49] = __bfloat162float(a.save_a2[((size_t)b * 81 + pos) * 32 + c]);
         }
-        for (int k = tid; k < 25 * 32; k += kThreads) {
+        for (int k = tid; k < 25 * 32; k += kBwdThreads) {
             const int p = k >> 5, c = k & 31;
             z3[c * 25 + p] = a.save_a3[(size_t)b * 800 + k];
         }
@@ -662,7 +664,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_prop_bwd(BwdArgs a)
         }
         __syncthreads();
         // ---- head ----
-        for (int f = tid; f < 800; f += kThreads) {
+        for (int f = tid; f < 800; f += kBwdThreads) {
             const float act = z3[f];  // [channel][position] flattening, as the head's
             float da = 0.f;
 #pragma unroll
@@ -675,7 +677,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_prop_bwd(BwdArgs a)
         if (tid < NOUT) g[kWH + NOUT * 800 + tid] += dO[tid];
         __syncthreads();
         // ---- conv3: weight gradients ----
-        for (int k = tid; k < 1024; k += kThreads) {
+        for (int k = tid; k < 1024; k += kBwdThreads) {
             const int co = k & 31, ci = k >> 5;
             float acc[9];
 #pragma unroll
@@ -696,7 +698,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_prop_bwd(BwdArgs a)
             g[kB3 + tid] += s;
         }
         // ---- conv3: input gradient, ReLU mask -> dz2 ----
-        for (int k = tid; k < 32 * 49; k += kThreads) {
+        for (int k = tid; k < 32 * 49; k += kBwdThreads) {
             const int ci = k / 49, qp = k - ci * 49, iy = qp / 7, ix = qp - iy * 7;
             float s = 0.f;
             if (a2[ci * 49 + qp] > 0.f) {
@@ -714,7 +716,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_prop_bwd(BwdArgs a)
         }
         __syncthreads();
         // ---- conv2: weight gradients ----
-        for (int k = tid; k < 512; k += kThreads) {
+        for (int k = tid; k < 512; k += kBwdThreads) {
             const int co = k & 31, ci = k >> 5;
             float acc[9];
 #pragma unroll
@@ -735,7 +737,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_prop_bwd(BwdArgs a)
             g[kB2 + tid] += s;
         }
         // ---- conv2: input gradient, ReLU mask -> dz1 ----
-        for (int k = tid; k < 16 * 81; k += kThreads) {
+        for (int k = tid; k < 16 * 81; k += kBwdThreads) {
             const int ci = k / 81, qp = k - ci * 81, iy = qp / 9, ix = qp - iy * 9;
             float s = 0.f;
             if (a1[ci * 81 + qp] > 0.f) {
@@ -753,6 +755,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_prop_bwd(BwdArgs a)
         }
         __syncthreads();
         // ---- conv1: weight gradients ----
+        static_assert(kBwdThreads >= 160, "one thread per conv1 weight and bias");
         if (tid < 144) {
             const int co = tid / 9, t = tid - co * 9, dy = t / 3, dx = t % 3;
             float s = 0.f;
@@ -766,7 +769,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_prop_bwd(BwdArgs a)
         }
         __syncthreads();
     }
-    for (int k = tid; k < L::NW; k += kThreads)
+    for (int k = tid; k < L::NW; k += kBwdThreads)
         if (g[k] != 0.f) atomicAdd(&a.grad[k], g[k]);
     if (tid < NOUT) atomicAdd(a.loss, lsum);
 }
@@ -876,7 +879,7 @@ template <int NOUT> cudaError_t launch_bwd(const BwdArgs &a, int grid, cudaStrea
         attr_err = cudaFuncSetAttribute(k_prop_bwd<NOUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     });
     if (attr_err != cudaSuccess) return attr_err;
-    k_prop_bwd<NOUT><<<grid, kThreads, bytes, stream>>>(a);
+    k_prop_bwd<NOUT><<<grid, kBwdThreads, bytes, stream>>>(a);
     return cudaGetLastError();
 }
 
@@ -917,7 +920,7 @@ cudaError_t enqueue_proposal(const ProposalView &net, const uint16_t *frames, lo
     a.err = err;
     const int groups = (n + kR - 1) / kR;
     const int sms = sm_count(net.device);
-    const int grid = groups < sms ? groups : sms;
+    const int grid = groups < kCtasPerSm * sms ? groups : kCtasPerSm * sms;
     if (launches) ++*launches;
     switch (nout) {
     case 5: return launch_fwd<5, 1>(a, grid, stream);
@@ -1030,7 +1033,7 @@ int forward_stack(loc_proposal *p, const uint16_t *d_rois, const int *d_index, i
     }
     const int groups = (n + locb::kR - 1) / locb::kR;
     const int sms = locb::sm_count(p->device);
-    const int grid = groups < sms ? groups : sms;
+    const int grid = groups < locb::kCtasPerSm * sms ? groups : locb::kCtasPerSm * sms;
     cudaError_t e;
     switch (p->nout) {
     case 5: e = locb::launch_fwd<5, 0>(a, grid, st); break;
