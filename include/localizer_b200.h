@@ -217,6 +217,26 @@ LOC_API int loc_fit_host(loc_ctx *ctx, const uint16_t *frames, int n_frames, int
                          uint8_t *flags);
 
 /*
+ * The same fit for a stream of stacks (the reference's analysis keeps its
+ * worker threads busy on frame after frame, source/PALMAnalysis.cpp:126-130,
+ * 196-250): enqueues the upload, the fit and the download of one stack and
+ * returns without waiting. Calls run in order; the upload of a call overlaps
+ * the fit of the one before it and its download the fit of the one after
+ * it (two device slots used in turn). `frames`, `cands`, `out` and `flags`
+ * must stay valid, and `out`/`flags` unread, until loc_fit_host_wait
+ * returns; pinned host memory (cudaHostAlloc / cudaHostRegister) is needed
+ * for the copies to overlap. Make no other fit call on the context while
+ * calls are in flight. Results are identical to loc_fit_host's.
+ */
+LOC_API int loc_fit_host_async(loc_ctx *ctx, const uint16_t *frames, int n_frames, int n_rows,
+                               int n_cols, const loc_candidate *cands, int n_cands, int method,
+                               double w0, double sigma, const loc_options *opt, double *out,
+                               uint8_t *flags);
+/* Waits for every loc_fit_host_async call of the context; reports the first
+ * device error of those calls. */
+LOC_API int loc_fit_host_wait(loc_ctx *ctx);
+
+/*
  * Allocation-free form of loc_fit_batch (same arguments, no context, same
  * results). It has no counterpart in the reference, which fits on the CPU
  * and allocates freely; it exists for callers that may not allocate device

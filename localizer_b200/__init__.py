@@ -83,6 +83,9 @@ _PROTOS = {
                                 C.c_double, C.c_double, C.POINTER(Options), C.c_void_p, C.c_void_p, C.c_void_p]),
     "loc_fit_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                C.c_double, C.c_double, C.POINTER(Options), C.c_void_p, C.c_void_p]),
+    "loc_fit_host_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                     C.c_int, C.c_double, C.c_double, C.POINTER(Options), C.c_void_p, C.c_void_p]),
+    "loc_fit_host_wait": (C.c_int, [C.c_void_p]),
     "loc_fit_batch_static": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                        C.c_double, C.c_double, C.POINTER(Options), C.c_void_p, C.c_void_p,
                                        C.c_void_p]),
@@ -176,6 +179,7 @@ class Engine:
 
     def __init__(self, device: int = 0):
         self._h = C.c_void_p()
+        self._inflight = []
         _check(lib().loc_ctx_create(C.byref(self._h), device))
 
     def close(self):
@@ -227,6 +231,34 @@ class Engine:
         _check(lib().loc_fit_host(self._h, frames.ctypes.data, n_frames, n_rows, n_cols, cands.ctypes.data, n,
                                   method, w0, sigma, C.byref(o), out.ctypes.data, flags.ctypes.data))
         return out, flags
+
+    def fit_host_async(self, frames: np.ndarray, cands: np.ndarray, method: int, w0: float, sigma: float,
+                       out: np.ndarray, flags: np.ndarray, options: Options | None = None):
+        """loc_fit_host_async: enqueue the fit of one stack and return.
+        `frames` (n_frames, n_cols, n_rows) uint16, `cands` (CANDIDATE_DTYPE),
+        `out` (n, loc_output_columns) float64 and `flags` (n,) uint8 are
+        C-contiguous arrays, kept referenced here until wait(); page-locked
+        arrays let the copies overlap the fits."""
+        n_frames, n_cols, n_rows = frames.shape
+        n = len(cands)
+        ncol = _check(lib().loc_output_columns(method))
+        for a in (frames, cands, out, flags):
+            if not a.flags["C_CONTIGUOUS"]:
+                raise LocalizerError("fit_host_async needs C-contiguous arrays")
+        if frames.dtype.itemsize != 2 or cands.dtype != CANDIDATE_DTYPE or out.shape != (n, ncol) or \
+                out.dtype != np.float64 or flags.shape != (n,) or flags.dtype != np.uint8:
+            raise LocalizerError("fit_host_async: array types or shapes do not match the call")
+        o = options if options is not None else default_options()
+        self._inflight.append((frames, cands, out, flags, o))
+        _check(lib().loc_fit_host_async(self._h, frames.ctypes.data, n_frames, n_rows, n_cols, cands.ctypes.data,
+                                        n, method, w0, sigma, C.byref(o), out.ctypes.data, flags.ctypes.data))
+
+    def wait(self):
+        """loc_fit_host_wait: block until every fit_host_async call is done."""
+        try:
+            _check(lib().loc_fit_host_wait(self._h))
+        finally:
+            self._inflight = []
 
 
 _default_engine = None

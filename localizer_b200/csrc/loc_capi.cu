@@ -73,6 +73,15 @@ struct loc_ctx {
     cudaStream_t aux[locb::kMaxAux] = {};
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[locb::kMaxAux] = {};
+    // loc_fit_host_async: two device slots used in turn, and one stream each
+    // for uploads, fits and downloads, so that a call's upload runs while the
+    // previous call fits and its download while the next call fits
+    struct HostSlot {
+        DevBuf frames, cands, out, flags;
+        cudaEvent_t in_done = nullptr, fit_done = nullptr, out_done = nullptr;
+    } slot[2];
+    int next_slot = 0;
+    cudaStream_t s_in = nullptr, s_fit = nullptr, s_out = nullptr;
 };
 
 extern "C" {
@@ -158,6 +167,19 @@ LOC_API int loc_ctx_destroy(loc_ctx *ctx)
     for (int k = 0; k < locb::kMaxAux; ++k) {
         if (ctx->aux[k]) cudaStreamDestroy(ctx->aux[k]);
         if (ctx->join[k]) cudaEventDestroy(ctx->join[k]);
+    }
+    for (cudaStream_t s : {ctx->s_in, ctx->s_fit, ctx->s_out})
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    for (auto &sl : ctx->slot) {
+        sl.frames.release();
+        sl.cands.release();
+        sl.out.release();
+        sl.flags.release();
+        for (cudaEvent_t ev : {sl.in_done, sl.fit_done, sl.out_done})
+            if (ev) cudaEventDestroy(ev);
     }
     delete ctx;
     return LOC_OK;
@@ -321,6 +343,8 @@ LOC_API int loc_fit_host(loc_ctx *ctx, const uint16_t *frames, int n_frames, int
 {
     int rc = validate(ctx, frames, n_frames, n_rows, n_cols, cands, n_cands, method, w0, sigma, out, flags);
     if (rc) return rc;
+    // asynchronous calls still in flight share the context's scratch
+    if ((rc = loc_fit_host_wait(ctx)) != LOC_OK) return rc;
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
     const size_t fbytes = (size_t)n_frames * n_rows * n_cols * sizeof(uint16_t);
@@ -346,6 +370,80 @@ LOC_API int loc_fit_host(loc_ctx *ctx, const uint16_t *frames, int n_frames, int
     if (n_cands && (e = cudaMemcpyAsync(flags, ctx->flags.p, n_cands, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return cuda_fail(e, "flags download");
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "fit");
+    return LOC_OK;
+}
+
+LOC_API int loc_fit_host_async(loc_ctx *ctx, const uint16_t *frames, int n_frames, int n_rows, int n_cols,
+                               const loc_candidate *cands, int n_cands, int method, double w0, double sigma,
+                               const loc_options *opt, double *out, uint8_t *flags)
+{
+    int rc = validate(ctx, frames, n_frames, n_rows, n_cols, cands, n_cands, method, w0, sigma, out, flags);
+    if (rc) return rc;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    if (!ctx->s_in) {
+        for (cudaStream_t *s : {&ctx->s_in, &ctx->s_fit, &ctx->s_out})
+            if ((e = cudaStreamCreateWithFlags(s, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(e, "stream");
+        for (auto &sl : ctx->slot)
+            for (cudaEvent_t *ev : {&sl.in_done, &sl.fit_done, &sl.out_done})
+                if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess)
+                    return cuda_fail(e, "event");
+    }
+    loc_ctx::HostSlot &sl = ctx->slot[ctx->next_slot];
+    const size_t fbytes = (size_t)n_frames * n_rows * n_cols * sizeof(uint16_t);
+    const size_t cbytes = (size_t)n_cands * sizeof(loc_candidate);
+    const int ncol = loc_output_columns(method);
+    const size_t obytes = (size_t)n_cands * ncol * sizeof(double);
+    loc_options o;
+    if (opt) o = *opt;
+    else loc_default_options(&o);
+    const size_t need = locb::scratch_bytes(method, n_cands, o.precision, o.fp64_rerun >= 0 ? 1 : 0,
+                                            o.proposal ? 1 : 0);
+    if (sl.frames.cap < fbytes || sl.cands.cap < cbytes || sl.out.cap < obytes || sl.flags.cap < (size_t)n_cands ||
+        ctx->scratch.cap < need) {
+        // a buffer grows: the calls in flight may still use the old one
+        if ((rc = loc_fit_host_wait(ctx)) != LOC_OK) return rc;
+        if ((e = sl.frames.ensure(fbytes ? fbytes : 1)) != cudaSuccess ||
+            (e = sl.cands.ensure(cbytes ? cbytes : 1)) != cudaSuccess ||
+            (e = sl.out.ensure(obytes ? obytes : 1)) != cudaSuccess ||
+            (e = sl.flags.ensure(n_cands ? n_cands : 1)) != cudaSuccess)
+            return fail(LOC_E_NOMEM, std::string("device buffers: ") + cudaGetErrorString(e));
+    }
+    // this slot's previous fit has read its frames and candidates
+    if ((e = cudaStreamWaitEvent(ctx->s_in, sl.fit_done, 0)) != cudaSuccess) return cuda_fail(e, "stream wait");
+    if (fbytes && (e = cudaMemcpyAsync(sl.frames.p, frames, fbytes, cudaMemcpyHostToDevice, ctx->s_in)) != cudaSuccess)
+        return cuda_fail(e, "frames upload");
+    if (cbytes && (e = cudaMemcpyAsync(sl.cands.p, cands, cbytes, cudaMemcpyHostToDevice, ctx->s_in)) != cudaSuccess)
+        return cuda_fail(e, "candidates upload");
+    if ((e = cudaEventRecord(sl.in_done, ctx->s_in)) != cudaSuccess) return cuda_fail(e, "event record");
+    // the fit waits for its upload and for the download of this slot's previous rows
+    if ((e = cudaStreamWaitEvent(ctx->s_fit, sl.in_done, 0)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(ctx->s_fit, sl.out_done, 0)) != cudaSuccess)
+        return cuda_fail(e, "stream wait");
+    if (n_cands > 0)
+        rc = loc_fit_batch(ctx, (const uint16_t *)sl.frames.p, n_frames, n_rows, n_cols,
+                           (const loc_candidate *)sl.cands.p, n_cands, method, w0, sigma, opt, (double *)sl.out.p,
+                           (uint8_t *)sl.flags.p, ctx->s_fit);
+    if ((e = cudaEventRecord(sl.fit_done, ctx->s_fit)) != cudaSuccess) return cuda_fail(e, "event record");
+    if (rc) return rc;
+    if ((e = cudaStreamWaitEvent(ctx->s_out, sl.fit_done, 0)) != cudaSuccess) return cuda_fail(e, "stream wait");
+    if (obytes && (e = cudaMemcpyAsync(out, sl.out.p, obytes, cudaMemcpyDeviceToHost, ctx->s_out)) != cudaSuccess)
+        return cuda_fail(e, "rows download");
+    if (n_cands && (e = cudaMemcpyAsync(flags, sl.flags.p, n_cands, cudaMemcpyDeviceToHost, ctx->s_out)) != cudaSuccess)
+        return cuda_fail(e, "flags download");
+    if ((e = cudaEventRecord(sl.out_done, ctx->s_out)) != cudaSuccess) return cuda_fail(e, "event record");
+    ctx->next_slot ^= 1;
+    return LOC_OK;
+}
+
+LOC_API int loc_fit_host_wait(loc_ctx *ctx)
+{
+    if (!ctx) return fail(LOC_E_INVALID, "ctx is NULL");
+    if (!ctx->s_in) return LOC_OK;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    for (cudaStream_t s : {ctx->s_in, ctx->s_fit, ctx->s_out})
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "host fit");
     return LOC_OK;
 }
 

@@ -129,6 +129,42 @@ def test_device_pointer_api_matches_host_api(engine):
     np.testing.assert_array_equal(d_out.cpu().numpy(), rows_h)
 
 
+def test_async_host_calls_match_host_call(engine):
+    """A stream of loc_fit_host_async calls over stacks of different sizes and
+    methods (slots reused and grown while calls are in flight) gives the rows
+    and flags loc_fit_host gives for each stack."""
+    import torch
+    jobs = []
+    for name, nf, method in (("uneven", 6, 7), ("uneven", 20, 7), ("small", 16, 0), ("uneven", 12, 5)):
+        w, frames, cands = _workload(name, nf, seed=300 + nf)
+        jobs.append((w, frames, cands, method))
+    jobs.append(jobs[0])
+    expect = [engine.fit_host(fr, c, m, w.w0) for w, fr, c, m in jobs]
+    outs = []
+    for k, (w, frames, cands, method) in enumerate(jobs):
+        n, ncol = len(cands), L.lib().loc_output_columns(method)
+        if k % 2:  # page-locked buffers for every other call
+            pf = torch.empty(frames.shape, dtype=torch.int16, pin_memory=True).numpy().view(np.uint16)
+            pf[...] = frames
+            frames = pf
+        out, flags = np.full((n, ncol), -7.0), np.full(n, 99, dtype=np.uint8)
+        engine.fit_host_async(frames, cands, method, w.w0, 1.0, out, flags)
+        outs.append((out, flags))
+    engine.wait()
+    for (rows, flags), (out, fl) in zip(expect, outs):
+        np.testing.assert_array_equal(fl, flags)
+        np.testing.assert_array_equal(out, rows)
+    # a synchronous call right after asynchronous ones finishes them first
+    w, frames, cands, method = jobs[1]
+    out, flags = np.zeros((len(cands), L.lib().loc_output_columns(method))), np.zeros(len(cands), np.uint8)
+    engine.fit_host_async(frames, cands, method, w.w0, 1.0, out, flags)
+    rows2, flags2 = engine.fit_host(frames, cands, method, w.w0)
+    np.testing.assert_array_equal(out, expect[1][0])
+    np.testing.assert_array_equal(rows2, expect[1][0])
+    np.testing.assert_array_equal(flags2, expect[1][1])
+    engine.wait()
+
+
 def test_edge_cases(engine):
     g = G.load("small")
     frames = g["frames"]
