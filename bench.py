@@ -203,6 +203,85 @@ def run_reference_sample(frames_host, cands, w0, budget_s=12.0, threads=None):
     return len(sub) / dt, len(sub), len(ths), idx, rows, kept
 
 
+def measure_next_rows(eng, frames_dev, frames_host, cands, d_cands, w0, rows_plain, flags_plain, hbm_peak):
+    """Throughput of the path's neighbours on the same workload, outside the
+    timed region: frame ingest (row-major float32 camera frames -> the
+    uint16 stack, HBM-bound at 4 + 2 B per pixel), the MLEwG fit (method 6)
+    against the reference's own MLEwG on one host core, and the positions
+    text writer."""
+    import tempfile
+
+    import torch
+
+    import localizer_b200 as L
+    from oracle import oracle as O
+    out = {}
+    # ingest: 2000 frames (> L2), transposed and converted
+    nf = min(2000, frames_dev.shape[0])
+    src = (frames_dev[:nf].to(torch.int32) & 0xFFFF).to(torch.float32).transpose(1, 2).contiguous()
+    dst, lossy = L.ingest_frames(src, row_major=True)
+    assert lossy == 0 and torch.equal(dst, frames_dev[:nf])
+    reps = 10
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        L.ingest_frames(src, row_major=True)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    gbs = nf * src.shape[1] * src.shape[2] * 6 / (ms / 1e3) / 1e9
+    out["ingest"] = {"kernel": "k_ingest_rm<float>", "frames": nf, "ms_per_call": ms, "frames_per_s": nf / (ms / 1e3),
+                     "achieved_gbs": gbs, "peak_gbs": hbm_peak, "frac": gbs / hbm_peak,
+                     "bytes_per_pixel": 6, "check": "lossless round trip of the uint16 stack"}
+    del src, dst
+    # MLEwG on the first 100k candidates
+    k = min(100000, len(cands))
+    ncol6 = L.lib().loc_output_columns(6)
+    o6 = torch.empty((k, ncol6), dtype=torch.float64, device="cuda")
+    f6 = torch.empty(k, dtype=torch.uint8, device="cuda")
+    opt6 = L.default_options(max_half_width=int(cands["half_width"].max()))
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def fit6():
+        eng.fit_device(frames_dev.data_ptr(), frames_dev.shape[0], frames_dev.shape[2], frames_dev.shape[1],
+                       d_cands.data_ptr(), k, 6, w0, 1.0, o6.data_ptr(), f6.data_ptr(), stream, opt6)
+
+    fit6()
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(3):
+        fit6()
+    b.record()
+    torch.cuda.synchronize()
+    ms6 = a.elapsed_time(b) / 3
+    mlewg = {"candidates": k, "ms_per_call": ms6, "fits_per_s": k / (ms6 / 1e3)}
+    if O.ref_available():
+        f0 = int(cands["frame"][0])
+        sel = np.nonzero(cands["frame"][:k] == f0)[0]
+        t = time.perf_counter()
+        rout, rkept, _, _ = O.ref_fit(frames_host, np.ascontiguousarray(cands[sel]), 6, w0)
+        dt = time.perf_counter() - t
+        g = o6[torch.from_numpy(sel).cuda()].cpu().numpy()
+        gk = f6[torch.from_numpy(sel).cuda()].cpu().numpy() == 0
+        rk = rkept == 1
+        same = (gk == rk) & (~gk | np.all(g[:, :8] == rout[:, :8], axis=1))
+        mlewg["reference_one_core"] = {"fits_per_s": len(sel) / dt, "fits": int(len(sel)),
+                                       "sample": f"the {len(sel)} candidates of frame {f0}"}
+        mlewg["identical_to_reference"] = float(np.mean(same))
+    out["mlewg"] = mlewg
+    # writer: the plain fit's rows
+    m = min(300000, len(rows_plain))
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "positions.txt")
+        t = time.perf_counter()
+        kept = L.write_positions(path, rows_plain[:m], flags_plain[:m], METHOD, "bench")
+        dt = time.perf_counter() - t
+        size = os.path.getsize(path)
+    out["writer"] = {"rows": m, "kept_rows_written": int(kept), "s": dt, "rows_per_s": m / dt,
+                     "mb_per_s": size / dt / 1e6, "threads": os.cpu_count()}
+    return out
+
+
 def reference_arm(args):
     rank, world, local = dist_env()
     if rank != 0:
@@ -416,6 +495,11 @@ def main():
                                "position_within_1e-3px": float(np.mean(err < 1e-3)) if len(err) else None,
                                "position_max_err_px": float(err.max()) if len(err) else None}
 
+    next_rows = None
+    if rank == 0:
+        next_rows = measure_next_rows(eng, frames_dev, frames_host, cands, d_cands, w.w0,
+                                      outs["plain"][0].cpu().numpy(), outs["plain"][1].cpu().numpy(),
+                                      peaks.get("hbm_gbs", 6650.0))
     if rank == 0:
         sw = res["warm"]["stats"]
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -444,7 +528,8 @@ def main():
                              "flops_per_step": flops},
                 "proposal_roofline": prop_roof, "finder": finder,
                 "stats": st, "warm_stats": sw, "clocks": clocks, "warm_clocks": res["warm"]["clocks"], "e2e": e2e, "cpu_baseline": cpu,
-                "accuracy": accuracy, "gpu_launches": int(st["kernel_launches"]) * args.steps}
+                "accuracy": accuracy, "next_rows": next_rows,
+                "gpu_launches": int(st["kernel_launches"]) * args.steps}
         print(json.dumps(line))
     net.close()
     eng.close()

@@ -107,9 +107,29 @@ extern "C" LOC_API long long loc_ingest_frames(const void *d_src, int format, in
     if (n_frames > 65535 && row_major) return locb::record_error_fixed(LOC_E_UNSUPPORTED, "too many frames in one call");
     if (n_frames == 0) return 0;
     const cudaStream_t st = (cudaStream_t)stream;
-    unsigned long long *cnt = nullptr;
-    cudaError_t e = cudaMallocAsync((void **)&cnt, sizeof(unsigned long long), st);
+    // one lossy counter per host thread and device, kept across calls (a
+    // stream-ordered allocation per call would go back to the driver at every
+    // synchronisation)
+    struct Counter {
+        unsigned long long *p = nullptr;
+        int dev = -1;
+        ~Counter()
+        {
+            if (p) cudaFree(p);
+        }
+    };
+    static thread_local Counter counter;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess && counter.dev != dev) {
+        if (counter.p) cudaFree(counter.p);
+        counter.p = nullptr;
+        counter.dev = -1;
+        e = cudaMalloc((void **)&counter.p, sizeof(unsigned long long));
+        if (e == cudaSuccess) counter.dev = dev;
+    }
     if (e != cudaSuccess) return locb::record_error_fixed(LOC_E_NOMEM, "ingest counter");
+    unsigned long long *cnt = counter.p;
     cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), st);
     switch (format) {
     case 2: e = launch<int8_t>(d_src, d_dst, n_frames, n_rows, n_cols, row_major, cnt, st); break;
@@ -123,12 +143,10 @@ extern "C" LOC_API long long loc_ingest_frames(const void *d_src, int format, in
     case 10: e = launch<float>(d_src, d_dst, n_frames, n_rows, n_cols, row_major, cnt, st); break;
     case 11: e = launch<double>(d_src, d_dst, n_frames, n_rows, n_cols, row_major, cnt, st); break;
     default:
-        cudaFreeAsync(cnt, st);
         return locb::record_error_fixed(LOC_E_UNSUPPORTED, "unsupported storage format (4-bit types are not)");
     }
     unsigned long long h = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h, cnt, sizeof h, cudaMemcpyDeviceToHost, st);
-    cudaFreeAsync(cnt, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return locb::record_error_fixed(LOC_E_CUDA, (std::string("ingest: ") + cudaGetErrorString(e)).c_str());
     return (long long)h;

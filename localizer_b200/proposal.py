@@ -299,23 +299,22 @@ def train(method: int = 7, n_rois: int = 2_000_000, epochs: int = 8, batch: int 
     net = Proposal(method, device, seed)
     steps_per_epoch = max(len(tr) // batch, 1)
     total = steps_per_epoch * epochs
+    # loss tracked on a fixed batch of held-out windows (no weight update)
+    probe = hold[:batch].contiguous()
+    loss0 = net.gradient(rois, labels, lam, index=probe)[1]
     hist = []
     t1 = time.time()
     step = 0
     for ep in range(epochs):
         order = tr[torch.randperm(len(tr), generator=g).to(tr.device)]
-        run = 0.0
         for k in range(steps_per_epoch):
             cur = lr * 0.5 * (1.0 + math.cos(math.pi * step / total)) + 1e-5
-            want = (k == steps_per_epoch - 1)
-            loss = net.train_step(rois, labels, lam, cur, index=order[k * batch:(k + 1) * batch].contiguous(),
-                                  want_loss=want)
+            net.train_step(rois, labels, lam, cur, index=order[k * batch:(k + 1) * batch].contiguous(),
+                           want_loss=False)
             step += 1
-            if want:
-                run = loss
-        hist.append(run)
+        hist.append(net.gradient(rois, labels, lam, index=probe)[1])
         if log:
-            log(f"[proposal] epoch {ep + 1}/{epochs} loss {run:.4f}")
+            log(f"[proposal] epoch {ep + 1}/{epochs} held-out loss {hist[-1]:.4f}")
     torch.cuda.synchronize()
     t_train = time.time() - t1
     net.status()
@@ -329,7 +328,9 @@ def train(method: int = 7, n_rois: int = 2_000_000, epochs: int = 8, batch: int 
     ix, iy = roles.index(2), roles.index(3)
     rep = {"method": method, "windows": n_rois, "labelled": int(valid.sum().item()), "epochs": epochs,
            "batch": batch, "steps": step, "data_s": t_data, "train_s": t_train,
-           "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1], "loss_weights": lam.tolist(),
+           "loss_initial": loss0, "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1],
+           "loss_probe": f"weighted squared error on {len(probe)} held-out windows after each epoch",
+           "loss_weights": lam.tolist(),
            "holdout": int(len(h)),
            "holdout_pos_rms_px": float(np.sqrt(np.mean(err[:, ix] ** 2 + err[:, iy] ** 2) / 2)),
            "holdout_pos_median_px": float(np.median(np.maximum(err[:, ix], err[:, iy]))),

@@ -114,7 +114,8 @@ def test_training_lowers_loss_and_warm_start_saves_iterations(gpu):
     torch, P = gpu
     from localizer_b200 import synth
     net, rep = P.train(method=0, n_rois=400_000, epochs=6, batch=2048, seed=21)
-    assert rep["loss_last_epoch"] < 0.7 * rep["loss_first_epoch"], rep
+    assert rep["loss_last_epoch"] < 0.5 * rep["loss_initial"], rep
+    assert rep["loss_last_epoch"] <= 1.05 * rep["loss_first_epoch"], rep
     assert rep["holdout_pos_median_px"] < 0.1, rep
     # warm start on the small golden-style workload: symmetric PSF, method 0
     w = synth.scaled(synth.workloads()["small"], 48, seed=4242)
