@@ -22,10 +22,12 @@ def _expected(src_np, row_major):
 @pytest.mark.parametrize("dtype", ["int8", "uint8", "int16", "uint16", "int32", "uint32", "int64", "uint64",
                                    "float32", "float64"])
 @pytest.mark.parametrize("row_major", [False, True])
-def test_ingest_matches_reference_mapping(dtype, row_major):
+# (3, 45, 70): an odd side, single-pixel accesses; (3, 46, 70) and (2, 130, 196):
+# even sides, paired / quad accesses; all with partial 64 x 64 transpose tiles
+@pytest.mark.parametrize("shape", [(3, 45, 70), (3, 46, 70), (2, 130, 196)])
+def test_ingest_matches_reference_mapping(dtype, row_major, shape):
     import torch
-    rng = np.random.default_rng(sum(map(ord, dtype)) * 2 + int(row_major))
-    shape = (3, 45, 70)                 # odd sizes: partial transpose tiles
+    rng = np.random.default_rng(sum(map(ord, dtype)) * 2 + int(row_major) + shape[1])
     info = np.iinfo(dtype) if dtype.startswith(("int", "uint")) else None
     lo = max(info.min, -300) if info else -300.0
     hi = min(info.max, 70000) if info else 70000.0
