@@ -217,7 +217,9 @@ __device__ __forceinline__ void pass_sym(const float *__restrict__ roi, int ld, 
         const T krow = -dxs * dxs - dys * (T(2) * wy + dys);  // (d2' - d2) minus its u term
         const float *row = roi + j * s * ld;
         if (S > 0) {
-#pragma unroll
+            // two columns per trip: unrolling all of them made the per-class
+            // solver large enough to miss in the instruction cache
+#pragma unroll 2
             for (int t = 0; t < (S > 0 ? (S + TPF - 1) / TPF : 1); ++t) {
                 const int i = q + TPF * t;
                 if (TPF == 1 || i < S) body(i, wy, wy2, krow, row);
@@ -275,7 +277,9 @@ __device__ __forceinline__ void pass_fixed(const float *__restrict__ roi, int ld
         const T krow = -dxs * dxs - dys * (T(2) * wy + dys);
         const float *row = roi + j * s * ld;
         if (S > 0) {
-#pragma unroll
+            // two columns per trip: unrolling all of them made the per-class
+            // solver large enough to miss in the instruction cache
+#pragma unroll 2
             for (int t = 0; t < (S > 0 ? (S + TPF - 1) / TPF : 1); ++t) {
                 const int i = q + TPF * t;
                 if (TPF == 1 || i < S) body(i, wy, wy2, krow, row);
@@ -373,7 +377,9 @@ __device__ __forceinline__ void pass_ell(const float *__restrict__ roi, int ld, 
                        T(2) * rb0 * dxs * wcur;
         const float *row = roi + j * s * ld;
         if (S > 0) {
-#pragma unroll
+            // two columns per trip: unrolling all of them made the per-class
+            // solver large enough to miss in the instruction cache
+#pragma unroll 2
             for (int t = 0; t < (S > 0 ? (S + TPF - 1) / TPF : 1); ++t) {
                 const int i = q + TPF * t;
                 if (TPF == 1 || i < S) body(i, wy, wy2, wc, wrb, brow, crow, row);
