@@ -541,41 +541,49 @@ __device__ __forceinline__ void lmpar_scaled(const T (&Ms)[tri(P)], const T (&g)
     const T idelta = frcp(delta);
     T dxnorm, w2, mp;
     singular = false;
-    ++n_lambda;
-    int rc = damped_solve<P, T>(Ms, T(0), g, thr, z, dxnorm, w2, newton_piv, n_esc);
-    bool rank_def = false;
-    if (rc != 0) {  // Newton step undefined: treat as infinitely long, no lower bound
-        rank_def = true;
-        dxnorm = (T)INFINITY;
-        w2 = T(0);
-        newton_piv = T(0);
-    }
-    T fp = dxnorm - delta;
-    if (!rank_def) margin = fmin(margin, fabs(fp - T(0.1) * delta) * idelta);
-    if (!rank_def && fp <= T(0.1) * delta) {
-        par = T(0);
-        return;
-    }
-    T par_l = (!rank_def && w2 > T(0)) ? fdiv(fp * idelta, w2) : T(0);
-    T gn2 = T(0);
-#pragma unroll
-    for (int i = 0; i < P; ++i) gn2 += g[i] * g[i];
-    const T gnorm = fsqrt(gn2);
-    T par_u = gnorm * idelta;
-    if (par_u == T(0)) par_u = tiny_pos<T>() / (delta < T(0.1) ? delta : T(0.1));
-    T pr = par;
-    if (pr > par_u) pr = par_u;
-    else if (pr < par_l) pr = par_l;
-    if (pr == T(0)) pr = fdiv(gnorm, dxnorm);
-    int fails = 0;
+    // One call site for the damped solve: the first trip is the undamped
+    // (Newton) solve, the others the lambda search (an inlined solve per call
+    // site would double the solver's code).
+    T fp = T(0), par_l = T(0), par_u = T(0), gnorm = T(0), pr = T(0);
+    bool first = true;
+    int fails = 0, it = 1;
 #pragma unroll 1
-    for (int it = 1;; ++it) {
-        if (pr == T(0)) {
+    for (;;) {
+        if (!first && pr == T(0)) {
             const T t = T(0.001) * par_u;
             pr = t > tiny_pos<T>() ? t : tiny_pos<T>();
         }
         ++n_lambda;
-        rc = damped_solve<P, T>(Ms, pr, g, thr, z, dxnorm, w2, mp, n_esc);
+        const int rc = damped_solve<P, T>(Ms, pr, g, thr, z, dxnorm, w2, mp, n_esc);
+        if (first) {
+            first = false;
+            newton_piv = mp;
+            bool rank_def = false;
+            if (rc != 0) {  // Newton step undefined: treat as infinitely long, no lower bound
+                rank_def = true;
+                dxnorm = (T)INFINITY;
+                w2 = T(0);
+                newton_piv = T(0);
+            }
+            fp = dxnorm - delta;
+            if (!rank_def) margin = fmin(margin, fabs(fp - T(0.1) * delta) * idelta);
+            if (!rank_def && fp <= T(0.1) * delta) {
+                par = T(0);
+                return;
+            }
+            par_l = (!rank_def && w2 > T(0)) ? fdiv(fp * idelta, w2) : T(0);
+            T gn2 = T(0);
+#pragma unroll
+            for (int i = 0; i < P; ++i) gn2 += g[i] * g[i];
+            gnorm = fsqrt(gn2);
+            par_u = gnorm * idelta;
+            if (par_u == T(0)) par_u = tiny_pos<T>() / (delta < T(0.1) ? delta : T(0.1));
+            pr = par;
+            if (pr > par_u) pr = par_u;
+            else if (pr < par_l) pr = par_l;
+            if (pr == T(0)) pr = fdiv(gnorm, dxnorm);
+            continue;
+        }
         if (rc != 0) {
             // the unit-diagonal scaled matrix plus a larger shift factorises
             if (++fails > 16) {
@@ -583,7 +591,6 @@ __device__ __forceinline__ void lmpar_scaled(const T (&Ms)[tri(P)], const T (&g)
                 break;
             }
             pr = pr * T(4) > T(1e-6) ? pr * T(4) : T(1e-6);
-            --it;
             continue;
         }
         const T fp_old = fp;
@@ -600,6 +607,7 @@ __device__ __forceinline__ void lmpar_scaled(const T (&Ms)[tri(P)], const T (&g)
             if (pr < par_u) par_u = pr;
         }
         pr = (par_l > pr + par_c) ? par_l : pr + par_c;
+        ++it;
     }
     par = pr;
 }
