@@ -343,7 +343,7 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
     auto theta_abs = [&](int k, const T (&t)[P]) -> T {
         return k == IX ? t[k] + (T)xo : (k == IX + 1 ? t[k] + (T)yo : t[k]);
     };
-    auto finish = [&](int status) {
+    auto write_finish = [&](int status) {
         if (leader) {
             T *o = (T *)a.state + (size_t)cidx * a.state_stride;
 #pragma unroll
@@ -369,10 +369,9 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
             st[ST_FITS] += 1;
             st[ST_ITERS] += iterations;
         }
-        phase = 0;
     };
     // park a fit that used up the first level's iteration budget
-    auto suspend = [&]() {
+    auto write_suspend = [&]() {
         if (leader) {
             float *o = a.cont_state + (size_t)cidx * a.cont_stride;
 #pragma unroll
@@ -399,7 +398,23 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
             const int slot = atomicAdd(a.meta + m_ccount(r), 1);
             a.cont[cstart + slot] = cidx;
         }
+    };
+    // finish() and suspend() only mark the fit; its state is written at the
+    // next flush(), before the lane is refilled (one inlined copy of each
+    // write-out instead of one per call site)
+    int done = -1;   // -1 nothing pending, -2 suspended, else the termination status
+    auto finish = [&](int status) {
+        done = status;
         phase = 0;
+    };
+    auto suspend = [&]() {
+        done = -2;
+        phase = 0;
+    };
+    auto flush = [&]() {
+        if (done == -2) write_suspend();
+        else if (done >= 0) write_finish(done);
+        done = -1;
     };
     auto test_delta = [&]() -> bool {
         bool ok = true;
@@ -440,6 +455,7 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
         t_mark = t;
     };
     while (true) {
+        flush();
         // ---- refill idle groups from the queue: one atomic per warp ----
         const bool want = (phase == 0) && !exhausted;
         const unsigned need = __ballot_sync(kFull, want && leader);
@@ -727,6 +743,7 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
         __syncwarp();
         lap(c_decide);
     }
+    flush();
     if (lane == 0) {
         st[ST_CYC_REFILL] += (unsigned)(c_refill >> 10);
         st[ST_CYC_STEP] += (unsigned)(c_step >> 10);
