@@ -500,10 +500,12 @@ template <int P, typename T>
 __device__ __forceinline__ int damped_solve(const T (&Ms)[tri(P)], T par, const T (&g)[P], float thr,
                                             T (&z)[P], T &znorm, T &w2, T &minpiv, unsigned &n_esc)
 {
-    int rc = chol_solve<P, T, T>(Ms, par, g, (T)thr, z, znorm, w2, minpiv);
-    if (rc == 1) {
-        ++n_esc;
-        if constexpr (sizeof(T) == 4) {
+    // FP64 solves take no pivot threshold (there is no higher precision to
+    // escalate to), so only FP32 solves can return 1
+    int rc = chol_solve<P, T, T>(Ms, par, g, sizeof(T) == 4 ? (T)thr : T(0), z, znorm, w2, minpiv);
+    if constexpr (sizeof(T) == 4) {
+        if (rc == 1) {
+            ++n_esc;
             float msl[tri(P)], gl[P], zl[P], o2[2];
 #pragma unroll
             for (int k = 0; k < tri(P); ++k) msl[k] = Ms[k];
@@ -514,9 +516,6 @@ __device__ __forceinline__ int damped_solve(const T (&Ms)[tri(P)], T par, const 
             for (int k = 0; k < P; ++k) z[k] = zl[k];
             znorm = o2[0];
             w2 = o2[1];
-        } else {
-            T mp2;
-            rc = chol_solve<P, double, T>(Ms, par, g, 0.0, z, znorm, w2, mp2);
         }
     }
     return rc;
