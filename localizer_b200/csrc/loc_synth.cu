@@ -6,7 +6,9 @@
 // f*n_rows*n_cols + x + y*n_rows.
 //
 // One block renders a 16 x 16 tile of one frame; the frame's emitters whose
-// 5-sigma box touches the tile are filtered into shared memory first.
+// 5-sigma box touches the tile are filtered into shared memory first, in
+// emitter order (at most 1024 per tile), so a seed gives the same frames on
+// every run.
 #include "../../include/localizer_b200.h"
 
 #include <cuda_runtime.h>
@@ -22,7 +24,9 @@ constexpr int kMaxLocal = 1024;
 __global__ void k5_render(uint16_t *frames, int n_rows, int n_cols, const float *em, const int *frame_start,
                           const float *background, float read_noise, unsigned long long seed)
 {
+    __shared__ float sem_raw[kMaxLocal * 5];
     __shared__ float sem[kMaxLocal * 5];
+    __shared__ int sidx[kMaxLocal];
     __shared__ int scount;
     const int f = blockIdx.z;
     const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
@@ -35,11 +39,23 @@ __global__ void k5_render(uint16_t *frames, int n_rows, int n_cols, const float 
         const float rx = 5.0f * sx + 1.0f, ry = 5.0f * sy + 1.0f;
         if (x + rx < tx0 || x - rx > tx0 + kTile - 1 || y + ry < ty0 || y - ry > ty0 + kTile - 1) continue;
         const int slot = atomicAdd(&scount, 1);
-        if (slot < kMaxLocal)
-            for (int q = 0; q < 5; ++q) sem[5 * slot + q] = em[5 * k + q];
+        if (slot < kMaxLocal) {
+            sidx[slot] = k;
+            for (int q = 0; q < 5; ++q) sem_raw[5 * slot + q] = em[5 * k + q];
+        }
     }
     __syncthreads();
     const int n = scount < kMaxLocal ? scount : kMaxLocal;
+    // emitters back into index order (each goes to the count of smaller
+    // indices), so that the expected counts are summed in the same order on
+    // every run and the frames are reproducible bit for bit
+    for (int t = tid; t < n; t += kTile * kTile) {
+        const int kk = sidx[t];
+        int rank = 0;
+        for (int j = 0; j < n; ++j) rank += sidx[j] < kk ? 1 : 0;
+        for (int q = 0; q < 5; ++q) sem[5 * rank + q] = sem_raw[5 * t + q];
+    }
+    __syncthreads();
     const int px = tx0 + threadIdx.x, py = ty0 + threadIdx.y;
     if (px >= n_rows || py >= n_cols) return;
     float lam = background[f];

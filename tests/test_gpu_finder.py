@@ -68,3 +68,17 @@ def test_gpu_finder_edge_cases():
     part, n = _gpu(g["frames"], 30.0, float(g["w0"]), cap=10)
     assert n == len(host)
     _same(part, host[:10])
+
+
+@pytest.mark.parametrize("name,n_frames", [("uneven", 300), ("stress", 200)])
+def test_device_synthesis_is_reproducible(name, n_frames):
+    """Frames rendered on the GPU (the bench's workload) are identical across
+    renders of the same seed, and so are the candidates found in them."""
+    import torch
+    w = synth.scaled(synth.workloads()[name], n_frames, seed=77)
+    a, _ = synth.make_device(w)
+    b, _ = synth.make_device(w)
+    assert torch.equal(a, b)
+    ca, na = L.find_candidates_device(a, 30.0, w.w0)
+    cb, nb = L.find_candidates_device(b, 30.0, w.w0)
+    assert na == nb and torch.equal(ca, cb)
