@@ -542,8 +542,10 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
                 }
             }
             __syncwarp();
-            if (phase == 3) start_iteration();
         }
+        // fits resumed from level 0 and fits whose last step was accepted
+        // start their next outer iteration here (one inlined copy of it)
+        if (phase == 3) start_iteration();
         if (__ballot_sync(kFull, phase != 0) == 0) break;
         lap(c_refill);
 
@@ -661,7 +663,7 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
                 par = T(0);
                 it_state = 1;
                 iterations = 0;
-                start_iteration();
+                phase = 3;  // next outer iteration, started after the refill
             } else {
                 T actred = T(-1);
                 if (T(0.1) * fn1 < fnorm) {
@@ -720,7 +722,7 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
                     }
                     if (test_delta()) finish(T_CONVERGED);
                     else if (iterations >= a.max_iter) finish(T_MAX_ITER);
-                    else start_iteration();
+                    else phase = 3;
                 } else {
                     T gmax = T(0);
 #pragma unroll
