@@ -324,7 +324,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames", type=int, default=10000)
-    ap.add_argument("--e2e-steps", type=int, default=6)
+    ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--ref-budget", type=float, default=12.0, help="seconds of CPU work per reference step")
     ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -470,7 +470,7 @@ def main():
            "h2d_bytes_per_step": int(frames_host.nbytes + cands.nbytes),
            "d2h_bytes_per_step": int(n * ncol * 8 + n), "arm": "plain",
            "call": "loc_fit_host_async per step (pinned host buffers; a step's upload overlaps the previous step's "
-                   "fit), loc_fit_host_wait at the end",
+                   "fit), loc_fit_host_wait at the end", "steps": args.e2e_steps,
            "one_call_per_step_value": e2e_sync}
     rows_e2e = ph_out.numpy().copy()
     flags_e2e = ph_flags.numpy().copy()
