@@ -1071,12 +1071,14 @@ cudaError_t launch_k1_tpf(const K1Args &ka, int r, int tpb, int bps_req, cudaStr
 }
 
 // One persistent solver launch for the queue of half-width r with tpf
-// threads per fit (1, 4 or 8 for FP32; 1 or 8 for FP64).
+// threads per fit (1, 4 or 8 for FP32; 1, 2, 4 or 8 for FP64).
 template <int METHOD, typename T>
 cudaError_t launch_k1(const K1Args &ka, int r, int tpb, int bps_req, int tpf, cudaStream_t stream)
 {
     if constexpr (sizeof(T) == 8) {
-        return tpf == 8 ? launch_k1_tpf<METHOD, T, 8>(ka, r, tpb, bps_req, stream)
+        return tpf == 4 ? launch_k1_tpf<METHOD, T, 4>(ka, r, tpb, bps_req, stream)
+             : tpf == 8 ? launch_k1_tpf<METHOD, T, 8>(ka, r, tpb, bps_req, stream)
+             : tpf == 2 ? launch_k1_tpf<METHOD, T, 2>(ka, r, tpb, bps_req, stream)
                         : launch_k1_tpf<METHOD, T, 1>(ka, r, tpb, bps_req, stream);
     } else {
         switch (tpf) {

@@ -48,7 +48,7 @@ struct FitParams {
     int tail_threads_per_fit;  // level 1: 1, 4 or 8
     int level0_budget;         // iterations before a fit moves to level 1 (0: single level)
     int fp64_rerun;            // re-run flagged FP32 fits in FP64
-    int rerun_threads_per_fit; // 1 or 8
+    int rerun_threads_per_fit; // 1, 2, 4 or 8
     float rerun_margin;        // branch-decision margin below which a fit is flagged
     float rerun_pivot;         // undamped pivot ratio below which a fit is flagged
     const float *init_params;
