@@ -144,8 +144,8 @@ typedef struct loc_options {
                                   -1: never */
     float rerun_margin;        /* 0: default 1e-4 */
     float rerun_pivot;         /* 0: default 1e-4 */
-    int32_t rerun_threads_per_fit; /* threads per fit of the FP64 re-run: 4
-                                  (default), 1, 2 or 8 */
+    int32_t rerun_threads_per_fit; /* threads per fit of the FP64 re-run: 2
+                                  (default), 1, 4 or 8 */
     int32_t serial_classes;    /* 0 (default): the ROI classes are solved as
                                   concurrent chains on the context's auxiliary
                                   streams, joined back to the call's stream;

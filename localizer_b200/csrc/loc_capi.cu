@@ -250,8 +250,8 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     p.tail_threads_per_fit = o.tail_threads_per_fit > 0 ? o.tail_threads_per_fit : 8;
     p.level0_budget = o.level0_budget == 0 ? 32 : (o.level0_budget < 0 ? 0 : o.level0_budget);
     p.fp64_rerun = rerun;
-    p.rerun_threads_per_fit = (o.rerun_threads_per_fit == 1 || o.rerun_threads_per_fit == 2 ||
-                               o.rerun_threads_per_fit == 8) ? o.rerun_threads_per_fit : 4;
+    p.rerun_threads_per_fit = (o.rerun_threads_per_fit == 1 || o.rerun_threads_per_fit == 4 ||
+                               o.rerun_threads_per_fit == 8) ? o.rerun_threads_per_fit : 2;
     p.rerun_margin = o.rerun_margin > 0 ? o.rerun_margin : 1e-4f;
     p.rerun_pivot = o.rerun_pivot > 0 ? o.rerun_pivot : 1e-4f;
     if (!(p.threads_per_fit == 1 || p.threads_per_fit == 4 || p.threads_per_fit == 8) ||

@@ -130,8 +130,8 @@ extern "C" LOC_API int loc_fit_batch_static(const uint16_t *d_frames, int n_fram
     p.tail_threads_per_fit = tpf1;
     p.level0_budget = o.level0_budget == 0 ? 32 : (o.level0_budget < 0 ? 0 : o.level0_budget);
     p.fp64_rerun = rerun;
-    p.rerun_threads_per_fit = (o.rerun_threads_per_fit == 1 || o.rerun_threads_per_fit == 2 ||
-                               o.rerun_threads_per_fit == 8) ? o.rerun_threads_per_fit : 4;
+    p.rerun_threads_per_fit = (o.rerun_threads_per_fit == 1 || o.rerun_threads_per_fit == 4 ||
+                               o.rerun_threads_per_fit == 8) ? o.rerun_threads_per_fit : 2;
     p.rerun_margin = o.rerun_margin > 0 ? o.rerun_margin : 1e-4f;
     p.rerun_pivot = o.rerun_pivot > 0 ? o.rerun_pivot : 1e-4f;
     p.init_params = o.d_init_params;
