@@ -522,9 +522,11 @@ def main():
                                "proposal_ms": prop_ms, "solver_ms": res["warm"]["solver_ms"],
                                "training": train_rep},
                 "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                             "frac": achieved / peak, "traffic": 1537.0 * n,
+                             "frac": achieved / peak, "traffic": 304.0 * n,
                              "traffic_note": "DRAM bytes per step of the level-0 FP32 solver, scaled from the "
-                                             "ncu capture of 1000 frames (1537 B per fit, r = 6 class)",
+                                             "ncu capture of 1000 frames (r = 6 class: 13.4 MB read, 0 written "
+                                             "for about 44 k fits = 304 B per fit; ROI gather of 338 B per "
+                                             "13 x 13 ROI, partly from L2)",
                              "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 x max SM clock); "
                                             "no measured FP32 peak in MEASURED_PEAKS.json",
                              "kernel": "k1_lm_fit (plain arm, all classes and levels)", "kernel_ms": k_ms,
