@@ -69,3 +69,27 @@ def test_host_finder_matches_reference_finder(name):
     assert len(c) == len(ref)
     for k in ("x", "y", "intensity", "background", "frame"):
         assert np.array_equal(c[k], ref[k]), k
+
+
+def test_async_host_fit_checks_arrays_before_any_device_work():
+    """Engine.fit_host_async refuses buffers that do not match the call
+    (column count of the method, dtypes, contiguity) before the library
+    touches a device, so the checks run without a GPU."""
+    eng = object.__new__(L.Engine)   # no context: every call below must fail first
+    eng._h = C.c_void_p()
+    eng._inflight = []
+    frames = np.zeros((1, 16, 16), np.uint16)
+    cands = np.zeros(3, L.CANDIDATE_DTYPE)
+    ncol = L.lib().loc_output_columns(0)
+    good_out, good_flags = np.zeros((3, ncol)), np.zeros(3, np.uint8)
+    bad = [
+        (frames, cands, np.zeros((3, ncol - 1)), good_flags),             # wrong column count
+        (frames, cands, np.zeros((3, ncol), np.float32), good_flags),     # wrong row dtype
+        (frames, cands, good_out, np.zeros(2, np.uint8)),                 # wrong flag count
+        (frames, cands[::-1].copy().view(np.uint8).view(np.float64), good_out, good_flags),  # not candidates
+        (np.zeros((1, 16, 32), np.uint16)[:, :, ::2], cands, good_out, good_flags),          # not contiguous
+    ]
+    for fr, cd, out, fl in bad:
+        with pytest.raises(L.LocalizerError):
+            eng.fit_host_async(fr, cd, 0, 1.3, 1.0, out, fl)
+    assert eng._inflight == []
