@@ -1,32 +1,43 @@
 #!/usr/bin/env python
-"""Throughput of the B200 Gaussian-PSF fit engine (fits/s) on the batched,
-uneven-ROI workload: 10,000 frames of 256 x 256 uint16, 20-400 emitters per
-frame, ellipsoidal PSFs (sigma_x, sigma_y ~ U[1, 2] px), ROI half-width per
-candidate drawn from {3, 4, 5, 6}, amplitude lognormal (median 800),
-background U[50, 200], Poisson + Gaussian read noise (sigma 2 ADU), gain 1.
-Frames are generated on the GPU from seeded emitters; candidates come from
-the GLRT + adjacent-8 finder; every candidate is fitted by the ellipsoidal
-Gaussian method (code 7) in one persistent FP32 solver launch per step.
+"""Throughput of the B200 Gaussian-PSF fit engine (fits/s at the accuracy
+gate) on the synthetic workloads of the per-emitter localization path.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py [--config {1,2,3,5}] [--gpus N] [--steps K] [--warmup W]
+                    [--impl reference]
 
-One JSON line on rank 0. A step = one fit call over every candidate of the
-stack (frames and candidates resident in HBM). Two arms are timed on the same
-candidates: the plain LM (the reference's start values) and the
-learned-warm-start LM (a proposal network trained here on the GPU, before
-timing, on windows of separately seeded frames of the same workload; its
-cold-start fallback re-runs warm fits it judges unreliable with the
-reference start in FP64). The metric is fits/s at the accuracy gate
-(positions within 1e-3 px of the FP64 reference, >= 99.9 % flag agreement):
-`value` is the plain arm, the configuration that meets the gate on this
-workload (the warm-start arm is slower and misses the flag gate here: both
-arms' fits/s, their ratio and their accuracy on the reference sample are in
-the line). `e2e` runs the plain fit through the host-buffer C-ABI calls every step (frame and
-candidate upload from pinned host memory, fit, row and flag download): a stream
-of loc_fit_host_async calls, whose uploads overlap the previous step's fit, and,
-as `one_call_per_step_value`, the blocking loc_fit_host. The CPU
-reference arm runs the reference's own fitter (Localization.cpp compiled
-from the reference sources into oracle/_ref) on the host cores.
+Configurations (seeded synthetic frames, no dataset):
+
+  5 (default, the headline): large dense -- 50,000 frames of 512 x 512 uint16
+    resident in HBM (26.2 GB), 300-1000 emitters per frame, sigma_x, sigma_y
+    ~ U[1, 2] px, ROI half-width per candidate in {3, 4, 5, 6} (7/9/11/13
+    px), amplitude lognormal (median 800), background U[50, 200], Poisson +
+    read noise; symmetric (method 0) and ellipsoidal (method 7) fits
+    interleaved in alternating blocks of 5,000 frames.
+  1: plain method, small -- 512 frames of 128 x 128, 50 emitters per frame,
+    sigma 1.3, 9 x 9 ROI, method 0.
+  2: batched uneven -- 10,000 frames of 256 x 256, 20-400 emitters per frame,
+    ellipsoidal sigma U[1, 2], ROI half-width in {3, 4, 5, 6}, method 7.
+  3: precision stress -- 5,000 frames of 256 x 256, amplitude U[50, 200],
+    background 150, 10 % of emitters 1.5-3 px from a neighbour, sigma 1.5,
+    11 x 11 ROI, method 0; the line adds the FP32 / GPU-FP64 / CPU-FP64
+    precision report.
+
+Frames are rendered on the GPU from seeded emitters; candidates come from
+the GPU GLRT + adjacent-8 finder. A step fits every candidate of the stack
+(frames and candidates resident in HBM), one loc_fit_batch call per method.
+Two arms run on the same candidates: the plain LM (the reference's start
+values) and the learned-warm-start LM (a start-proposal network trained here
+on the GPU, before timing, on windows of separately seeded frames of the same
+workload type; warm fits it judges unreliable are re-run from the reference
+start in FP64). `value` is the plain arm; both arms' fits/s, their ratio and
+their accuracy against the reference's own fitter on a sample of the frames
+are in the line. `e2e` runs the plain fit through the host-buffer C-ABI
+calls (a stream of loc_fit_host_async calls from pinned host memory, one per
+block of frames, uploads overlapping the previous block's fit). The CPU
+reference arm (`--impl reference`) runs the reference's own fitter
+(Localization.cpp compiled from the reference sources into oracle/_ref) on
+all host cores, on frames of the same configuration rendered on the host,
+without loading this package's native library.
 """
 from __future__ import annotations
 
@@ -45,16 +56,36 @@ sys.path.insert(0, ROOT)
 
 METRIC = "fits/s at ≤1e-3 px vs FP64: learned-warm-start LM vs plain LM, 1 B200"
 UNIT = "fits/s"
-METHOD = 7                 # FitPositions_EllipsoidalGaussian
 PFA = 30.0
-# algorithmic FLOPs per ROI pixel: Jacobian evaluation (model, analytic
-# Jacobian, J^T J and J^T r accumulation) and trial evaluation, and per
-# damped p x p Cholesky solve (p^3/3 + 2 p^2), for the 7-parameter model
+# algorithmic FLOPs per ROI pixel of a Jacobian evaluation (model, analytic
+# Jacobian, J^T J and J^T r accumulation) and of a trial evaluation, and per
+# damped p x p Cholesky solve (p^3/3 + 2 p^2)
 FLOP_J = {0: 58, 1: 46, 5: 115, 7: 115}
 FLOP_F = 12
 NPAR = {0: 5, 1: 4, 5: 7, 7: 7}
 SM_COUNT = 148
 FP32_LANES = 128
+XCOL = {0: 3, 1: 2, 5: 4, 7: 4}
+# DRAM bytes per fit of the whole plain-arm solver chain (every kernel of the
+# step) from an ncu capture, or None while no capture of the current kernels
+# exists
+TRAFFIC_PER_FIT = None
+
+CONFIGS = {
+    1: {"workload": "small", "block": 0,
+        "label": "plain method, small: 512 frames 128x128 uint16, 50 emitters/frame, symmetric PSF sigma 1.3, "
+                 "9x9 ROI, method 0"},
+    2: {"workload": "uneven", "block": 0,
+        "label": "batched uneven: 10000 frames 256x256 uint16, 20-400 emitters/frame, ellipsoidal PSF sigma "
+                 "U[1,2], ROI half-width in {3,4,5,6}, method 7"},
+    3: {"workload": "stress", "block": 0,
+        "label": "precision stress: 5000 frames 256x256 uint16, 50 emitters/frame, amplitude U[50,200], "
+                 "background 150, 10% of emitters 1.5-3 px from a neighbour, sigma 1.5, 11x11 ROI, method 0"},
+    5: {"workload": "dense", "block": 5000,
+        "label": "large dense: 50000 frames 512x512 uint16 (26.2 GB resident), 300-1000 emitters/frame, "
+                 "sigma U[1,2], ROI 7/9/11/13, symmetric (method 0) and ellipsoidal (method 7) fits in "
+                 "alternating blocks of 5000 frames"},
+}
 
 
 def log(*a):
@@ -122,18 +153,42 @@ def dist_env():
     return rank, world, local
 
 
-def make_workload(n_frames: int, rank: int):
+def config_workload(cfg: int, n_frames: int | None, rank: int = 0):
+    """The configuration's workload (scaled to n_frames if given; each rank
+    its own seed) and its method block length in frames (0: one method)."""
+    from localizer_b200 import synth
+    c = CONFIGS[cfg]
+    base = synth.workloads()[c["workload"]]
+    nf = n_frames or base.n_frames
+    w = synth.scaled(base, nf, seed=base.seed + 7919 * rank)
+    block = c["block"]
+    if block and nf < base.n_frames:
+        block = max(1, nf // 10)
+    return w, block
+
+
+def method_of(w, block: int, frame: np.ndarray) -> np.ndarray:
+    """Fit method per candidate: the workload's method, or, for two methods,
+    the first on even blocks of `block` frames and the second on odd ones."""
+    if len(w.methods) == 1 or block <= 0:
+        return np.full(len(frame), w.methods[0], dtype=np.int32)
+    return np.where((frame // block) % 2 == 0, w.methods[0], w.methods[1]).astype(np.int32)
+
+
+def assign_half_widths(w, cands):
+    rng = np.random.default_rng(w.seed + 17)
+    cands["half_width"] = rng.choice(np.array(w.half_widths), size=len(cands))
+
+
+def make_workload(w):
+    """GPU-rendered frames and GPU-found candidates of a workload."""
     import torch
 
     import localizer_b200 as L
     from localizer_b200 import synth
-    w = synth.scaled(synth.workloads()["uneven"], n_frames, seed=1002 + 7919 * rank)
     t0 = time.time()
-    frames_dev, em = synth.make_device(w)
-    frames_host = frames_dev.cpu().numpy().view(np.uint16)
+    frames_dev, _ = synth.make_device(w)
     t1 = time.time()
-    # candidates from the GPU GLRT + adjacent-8 finder (bit-exact with the
-    # host finder), timed with CUDA events on its second run
     L.find_candidates_device(frames_dev, PFA, w.w0)
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s.record()
@@ -142,193 +197,203 @@ def make_workload(n_frames: int, rank: int):
     torch.cuda.synchronize()
     f_ms = s.elapsed_time(e)
     cands = raw.cpu().numpy().view(L.CANDIDATE_DTYPE).copy()
-    rng = np.random.default_rng(w.seed + 17)
-    cands["half_width"] = rng.choice(np.array(w.half_widths), size=len(cands))
-    finder = {"ms": f_ms, "frames_per_s": n_frames / (f_ms / 1e3), "candidates": int(n),
-              "frame_read_gbs": frames_host.nbytes / (f_ms / 1e3) / 1e9,
+    del raw
+    assign_half_widths(w, cands)
+    finder = {"ms": f_ms, "frames_per_s": w.n_frames / (f_ms / 1e3), "candidates": int(n),
+              "frame_read_gbs": frames_dev.numel() * 2 / (f_ms / 1e3) / 1e9,
               "kernels": "k_glrt, k_union, k_flatten, k_count_roots, k_assign, k_accumulate, k_emit"}
-    log(f"[bench] rank {rank}: {n_frames} frames rendered in {t1 - t0:.1f}s, {len(cands)} candidates found on the "
-        f"GPU in {f_ms:.1f} ms")
-    d_cands = torch.from_numpy(cands.view(np.uint8)).cuda()
-    return w, frames_dev, frames_host, cands, d_cands, finder
+    log(f"[bench] {w.n_frames} frames rendered in {t1 - t0:.1f}s, {len(cands)} candidates found on the GPU in "
+        f"{f_ms:.1f} ms")
+    return frames_dev, cands, finder
 
 
-def run_reference_sample(frames_host, cands, w0, budget_s=12.0, threads=None):
-    """The reference's own fitter (oracle/_ref) on a bounded, frame-aligned
-    sample of the workload, spread over host threads. Returns
-    (fits/s, n_fits, threads, sample indices, rows, kept)."""
+def ref_fit_parallel(frames_host, cands, methods, w0, threads):
+    """The reference's own fitter (oracle/_ref) over the candidates, whole
+    frames per host thread, one fitter call per (frame, half-width, method)
+    group as the reference's workers make them. Returns (seconds, rows per
+    method {m: (idx, rows, kept, iters)})."""
     from oracle import oracle as O
-    threads = threads or os.cpu_count() or 1
-    frame_ids = cands["frame"]
-    # calibrate on one frame
-    f0 = int(frame_ids[0])
-    sel = np.nonzero(frame_ids == f0)[0]
-    t = time.time()
-    O.ref_fit(frames_host, cands[sel], METHOD, 1.5)
-    per_fit = max((time.time() - t) / max(len(sel), 1), 1e-6)
-    n_target = int(budget_s * threads / per_fit)
-    # whole frames, evenly spaced through the stack
-    counts = np.bincount(frame_ids, minlength=frames_host.shape[0])
-    n_frames = frames_host.shape[0]
-    per_frame = max(counts.mean(), 1)
-    nf = int(min(n_frames, max(threads, n_target / per_frame)))
-    chosen = np.linspace(0, n_frames - 1, nf).astype(int)
-    chosen = np.unique(chosen)
-    mask = np.isin(frame_ids, chosen)
-    idx = np.nonzero(mask)[0]
-    sub = np.ascontiguousarray(cands[idx])
-    chunks = np.array_split(np.arange(len(chosen)), threads)
+    frame_ids = np.unique(cands["frame"])
+    chunks = [c for c in np.array_split(frame_ids, threads) if len(c)]
     results = [None] * len(chunks)
 
     def work(k):
-        fr = chosen[chunks[k]]
-        m = np.isin(sub["frame"], fr)
-        results[k] = (np.nonzero(m)[0], O.ref_fit(frames_host, np.ascontiguousarray(sub[m]), METHOD, 1.5))
+        m_sel = np.isin(cands["frame"], chunks[k])
+        part = {}
+        for m in np.unique(methods[m_sel]):
+            idx = np.nonzero(m_sel & (methods == m))[0]
+            out, kp, it, _ = O.ref_fit(frames_host, np.ascontiguousarray(cands[idx]), int(m), w0)
+            part[int(m)] = (idx, out, kp == 1, it)
+        results[k] = part
 
     t0 = time.perf_counter()
-    ths = [threading.Thread(target=work, args=(k,)) for k in range(len(chunks)) if len(chunks[k])]
+    ths = [threading.Thread(target=work, args=(k,)) for k in range(len(chunks))]
     for th in ths:
         th.start()
     for th in ths:
         th.join()
     dt = time.perf_counter() - t0
-    rows = np.full((len(sub), O.REF_COLUMNS[METHOD]), np.nan)
-    kept = np.zeros(len(sub), dtype=bool)
-    for r in results:
-        if r is None:
-            continue
-        ii, (out, kp, _, _) = r
-        rows[ii] = out
-        kept[ii] = kp == 1
-    return len(sub) / dt, len(sub), len(ths), idx, rows, kept
+    merged = {}
+    for part in results:
+        for m, (idx, out, kp, it) in part.items():
+            if m in merged:
+                a = merged[m]
+                merged[m] = (np.concatenate([a[0], idx]), np.concatenate([a[1], out]), np.concatenate([a[2], kp]),
+                             np.concatenate([a[3], it]))
+            else:
+                merged[m] = (idx, out, kp, it)
+    return dt, merged, len(chunks)
 
 
-def measure_next_rows(eng, frames_dev, frames_host, cands, d_cands, w0, rows_plain, flags_plain, hbm_peak):
-    """Throughput of the path's neighbours on the same workload, outside the
-    timed region: frame ingest (row-major float32 camera frames -> the
-    uint16 stack, HBM-bound at 4 + 2 B per pixel), the MLEwG fit (method 6)
-    against the reference's own MLEwG on one host core, and the positions
-    text writer."""
-    import tempfile
+def sample_frames(n_frames, per_frame, n_target, threads):
+    """Whole frames evenly spaced through the stack, about n_target fits."""
+    nf = int(min(n_frames, max(threads, n_target / max(per_frame, 1.0))))
+    return np.unique(np.linspace(0, n_frames - 1, nf).astype(int))
 
-    import torch
 
-    import localizer_b200 as L
+def calibrate_per_fit(frames_host, cands, methods, w0):
+    """Seconds per reference fit on one host thread, from one frame's fits."""
     from oracle import oracle as O
-    out = {}
-    # ingest: 2000 frames (> L2), transposed and converted
-    nf = min(2000, frames_dev.shape[0])
-    src = (frames_dev[:nf].to(torch.int32) & 0xFFFF).to(torch.float32).transpose(1, 2).contiguous()
-    dst, lossy = L.ingest_frames(src, row_major=True)
-    assert lossy == 0 and torch.equal(dst, frames_dev[:nf])
-    reps = 10
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record()
-    for _ in range(reps):
-        L.ingest_frames(src, row_major=True)
-    b.record()
-    torch.cuda.synchronize()
-    ms = a.elapsed_time(b) / reps
-    gbs = nf * src.shape[1] * src.shape[2] * 6 / (ms / 1e3) / 1e9
-    out["ingest"] = {"kernel": "k_ingest_rm<float>", "frames": nf, "ms_per_call": ms, "frames_per_s": nf / (ms / 1e3),
-                     "achieved_gbs": gbs, "peak_gbs": hbm_peak, "frac": gbs / hbm_peak,
-                     "bytes_per_pixel": 6, "check": "lossless round trip of the uint16 stack",
-                     "timing": "per call, including the call's host synchronisation for the lossy count",
-                     "peak_source": "hbm_gbs of measured MEASURED_PEAKS.json" if os.path.exists(
-                         os.path.join(ROOT, "MEASURED_PEAKS.json")) else "fallback 6.65 TB/s"}
-    del src, dst
-    # MLEwG on the first 100k candidates
-    k = min(100000, len(cands))
-    ncol6 = L.lib().loc_output_columns(6)
-    o6 = torch.empty((k, ncol6), dtype=torch.float64, device="cuda")
-    f6 = torch.empty(k, dtype=torch.uint8, device="cuda")
-    opt6 = L.default_options(max_half_width=int(cands["half_width"].max()))
-    stream = torch.cuda.current_stream().cuda_stream
+    f0 = int(cands["frame"][0])
+    sel = np.nonzero(cands["frame"] == f0)[0]
+    t = time.perf_counter()
+    for m in np.unique(methods[sel]):
+        s = sel[methods[sel] == m]
+        O.ref_fit(frames_host, np.ascontiguousarray(cands[s]), int(m), w0)
+    return max((time.perf_counter() - t) / max(len(sel), 1), 1e-6)
 
-    def fit6():
-        eng.fit_device(frames_dev.data_ptr(), frames_dev.shape[0], frames_dev.shape[2], frames_dev.shape[1],
-                       d_cands.data_ptr(), k, 6, w0, 1.0, o6.data_ptr(), f6.data_ptr(), stream, opt6)
 
-    fit6()
-    torch.cuda.synchronize()
-    a.record()
-    for _ in range(3):
-        fit6()
-    b.record()
-    torch.cuda.synchronize()
-    ms6 = a.elapsed_time(b) / 3
-    mlewg = {"candidates": k, "ms_per_call": ms6, "fits_per_s": k / (ms6 / 1e3)}
-    if O.ref_available():
-        f0 = int(cands["frame"][0])
-        sel = np.nonzero(cands["frame"][:k] == f0)[0]
-        t = time.perf_counter()
-        rout, rkept, _, _ = O.ref_fit(frames_host, np.ascontiguousarray(cands[sel]), 6, w0)
-        dt = time.perf_counter() - t
-        g = o6[torch.from_numpy(sel).cuda()].cpu().numpy()
-        gk = f6[torch.from_numpy(sel).cuda()].cpu().numpy() == 0
-        rk = rkept == 1
-        same = (gk == rk) & (~gk | np.all(g[:, :8] == rout[:, :8], axis=1))
-        mlewg["reference_one_core"] = {"fits_per_s": len(sel) / dt, "fits": int(len(sel)),
-                                       "sample": f"the {len(sel)} candidates of frame {f0}"}
-        mlewg["identical_to_reference"] = float(np.mean(same))
-    out["mlewg"] = mlewg
-    # writer: the plain fit's rows
-    m = min(300000, len(rows_plain))
-    with tempfile.TemporaryDirectory() as td:
-        path = os.path.join(td, "positions.txt")
-        t = time.perf_counter()
-        kept = L.write_positions(path, rows_plain[:m], flags_plain[:m], METHOD, "bench")
-        dt = time.perf_counter() - t
-        size = os.path.getsize(path)
-    out["writer"] = {"rows": m, "kept_rows_written": int(kept), "s": dt, "rows_per_s": m / dt,
-                     "mb_per_s": size / dt / 1e6, "threads": os.cpu_count()}
-    return out
+def accuracy_report(rows, flags, ref_rows, ref_kept, ref_iters, method):
+    """Flag agreement and position error against the reference fitter, with
+    the tail split by class: fits the reference stopped at its 200-iteration
+    cap (not converged) and fits it converged."""
+    gk = flags == 0
+    xi = XCOL[method]
+    both = gk & ref_kept
+    capped = ref_iters >= 200
+    rep = {"fits": int(len(flags)), "flag_agreement": float(np.mean(gk == ref_kept)) if len(flags) else None,
+           "flag_disagreements": int(np.sum(gk != ref_kept)), "jointly_kept": int(both.sum())}
+    for name, cls in (("converged", both & ~capped), ("reference_capped", both & capped)):
+        if cls.any():
+            err = np.abs(rows[cls, xi:xi + 2] - ref_rows[cls, xi:xi + 2]).max(axis=1)
+            rep[name] = {"n": int(cls.sum()), "position_within_1e-3px": float(np.mean(err < 1e-3)),
+                         "n_beyond_1e-3px": int(np.sum(err >= 1e-3)), "position_max_err_px": float(err.max()),
+                         "position_rms_err_px": float(np.sqrt(np.mean(err ** 2)))}
+        else:
+            rep[name] = {"n": 0}
+    return rep
 
 
 def reference_arm(args):
+    """The reference's own fitter on the host cores, on frames of the same
+    configuration rendered on the host (numpy) from the same seeded emitters
+    and candidates found by the reference's own GLRT + adjacent-8 pipeline
+    (oracle/_ref); no part of the native library is loaded."""
     rank, world, local = dist_env()
     if rank != 0:
         return 0
+    from localizer_b200 import synth
     from oracle import oracle as O
     if not O.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libloc_ref.so is absent"}))
         return 0
-    import torch
-    torch.cuda.set_device(local)
-    w, frames_dev, frames_host, cands, d_cands, _ = make_workload(args.frames, 0)
+    w, block = config_workload(args.config, args.frames)
+    threads = os.cpu_count() or 1
+    em, bg = synth.draw_stack(w)
+    per_frame = len(em.x) / w.n_frames
+    budget = args.ref_budget or float(np.clip(150.0 / (args.steps + args.warmup), 2.0, 12.0))
+    # calibrate on a few frames, then render the sample
+    probe = synth.render_frames(w, em, bg, [0], seed=w.seed)
+    pc = O.ref_find_candidates(probe, PFA, w.w0)
+    pc["half_width"] = np.random.default_rng(w.seed + 17).choice(np.array(w.half_widths), size=len(pc))
+    per_fit = calibrate_per_fit(probe, pc, method_of(w, block, np.zeros(len(pc), np.int64)), w.w0)
+    chosen = sample_frames(w.n_frames, per_frame, budget * threads / per_fit, threads)
+    t0 = time.time()
+    frames = np.empty((len(chosen), w.size, w.size), dtype=np.uint16)
+    found = [None] * threads
+    pieces = np.array_split(np.arange(len(chosen)), threads)
+
+    def prepare(k):
+        ii = pieces[k]
+        if len(ii) == 0:
+            return
+        frames[ii] = synth.render_frames(w, em, bg, chosen[ii], seed=w.seed)
+        c = O.ref_find_candidates(np.ascontiguousarray(frames[ii]), PFA, w.w0)
+        c["frame"] += ii[0]
+        found[k] = c
+
+    ths = [threading.Thread(target=prepare, args=(k,)) for k in range(threads)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    cands = np.concatenate([c for c in found if c is not None])
+    assign_half_widths(w, cands)
+    methods = method_of(w, block, chosen[cands["frame"]])
+    log(f"[bench reference] {len(chosen)} frames rendered and {len(cands)} candidates found on the host in "
+        f"{time.time() - t0:.1f}s; {budget:.1f}s of fits per step on {threads} threads")
     vals = []
+    th = threads
     for step in range(args.warmup + args.steps):
-        v, n, th, _, _, _ = run_reference_sample(frames_host, cands, w.w0, budget_s=args.ref_budget)
+        dt, _, th = ref_fit_parallel(frames, cands, methods, w.w0, threads)
         if step >= args.warmup:
-            vals.append(v)
+            vals.append(len(cands) / dt)
     value = float(np.mean(vals))
+    sample = (f"{len(cands)} candidates of {len(chosen)} whole frames spread through the stack per step "
+              f"(host-rendered from the configuration's seeded emitters); reference Localization.cpp FP64 + "
+              f"lmsder restatement, {th} threads")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * len(cands) / value, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; GPU-rendered frames)",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded emitters; host-rendered frames)",
             "impl": "reference",
-            "config": {"workload": "batched uneven: 10000 frames 256x256 uint16, 20-400 emitters/frame, "
-                                   "ellipsoidal PSF, ROI half-width in {3,4,5,6}", "frames": args.frames,
-                       "candidates": int(len(cands)), "method": METHOD},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": th, "kind": "reference",
-                             "sample": f"{n} candidates (whole frames spread through the stack) per step, "
-                                       f"reference Localization.cpp FP64 + lmsder restatement, {th} threads"},
+            "config": {"workload": CONFIGS[args.config]["label"], "config": args.config, "frames": w.n_frames,
+                       "sample_frames": int(len(chosen)), "sample_candidates": int(len(cands)),
+                       "methods": sorted(set(int(m) for m in w.methods))},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": th, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
 
 
+class Part:
+    """The candidates of one method: their device copy, an engine (its own
+    counters), and per-arm outputs."""
+
+    def __init__(self, L, torch, method, idx, cands, device):
+        self.method = method
+        self.idx = idx
+        self.cands = np.ascontiguousarray(cands[idx])
+        self.n = len(idx)
+        self.d_cands = torch.from_numpy(self.cands.view(np.uint8)).cuda()
+        self.eng = L.Engine(device)
+        self.ncol = L.lib().loc_output_columns(method)
+        self.outs = {}
+
+    def out(self, torch, arm):
+        if arm not in self.outs:
+            self.outs[arm] = (torch.empty((self.n, self.ncol), dtype=torch.float64, device="cuda"),
+                              torch.empty(self.n, dtype=torch.uint8, device="cuda"))
+        return self.outs[arm]
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--config", type=int, default=5, choices=sorted(CONFIGS))
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--frames", type=int, default=10000)
-    ap.add_argument("--e2e-steps", type=int, default=20)
-    ap.add_argument("--ref-budget", type=float, default=12.0, help="seconds of CPU work per reference step")
+    ap.add_argument("--frames", type=int, default=0, help="scale the configuration to this many frames")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="0: steps, at most 10")
+    ap.add_argument("--ref-budget", type=float, default=0.0, help="seconds of CPU work per reference step")
+    ap.add_argument("--ref-budget-repo", type=float, default=12.0,
+                    help="seconds of CPU work of the reference sample beside the GPU arms")
     ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--train-frames", type=int, default=4000, help="frames whose windows train the proposal")
+    ap.add_argument("--no-warm", action="store_true", help="plain arm only (profiling runs)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-next-rows", action="store_true")
+    ap.add_argument("--train-frames", type=int, default=3000, help="frames whose windows train each proposal")
     ap.add_argument("--train-epochs", type=int, default=8)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -347,200 +412,342 @@ def main():
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    w, frames_dev, frames_host, cands, d_cands, finder = make_workload(args.frames, rank)
+    w, block = config_workload(args.config, args.frames or None, rank)
+    frames_dev, cands, finder = make_workload(w)
     n = len(cands)
-    eng = L.Engine(local)
-    ncol = L.lib().loc_output_columns(METHOD)
-    stream = torch.cuda.current_stream()
+    methods = method_of(w, block, cands["frame"].astype(np.int64))
+    parts = [Part(L, torch, int(m), np.nonzero(methods == m)[0], cands, local) for m in w.methods
+             if np.any(methods == m)]
     n_frames, size = frames_dev.shape[0], frames_dev.shape[1]
-
-    # the proposal network, trained on the GPU by the library's own kernels
-    t_tr = time.time()
-    net, train_rep = PR.train(method=METHOD, n_rois=0, frames=args.train_frames, epochs=args.train_epochs,
-                              seed=7 + 1000 * rank, device=local)
-    train_rep["wall_s"] = time.time() - t_tr
-    log(f"[bench] rank {rank}: proposal trained in {train_rep['wall_s']:.1f}s "
-        f"({train_rep['labelled']} windows, holdout position median {train_rep['holdout_pos_median_px']:.3f} px)")
+    stream = torch.cuda.current_stream()
     mh = int(max(w.half_widths))
-    arms = {"plain": L.default_options(max_half_width=mh, precision=args.precision),
-            "warm": L.default_options(max_half_width=mh, precision=args.precision, proposal=net.handle.value)}
-    outs = {k: (torch.empty((n, ncol), dtype=torch.float64, device="cuda"),
-                torch.empty(n, dtype=torch.uint8, device="cuda")) for k in arms}
+
+    # the proposal networks (one per method), trained on the GPU by the library's own kernels
+    nets, train_rep = {}, {}
+    if not args.no_warm:
+        for p in parts:
+            t_tr = time.time()
+            net, rep = PR.train(method=p.method, n_rois=0, frames=args.train_frames, epochs=args.train_epochs,
+                                seed=7 + 1000 * rank, device=local, workload=CONFIGS[args.config]["workload"])
+            rep["wall_s"] = time.time() - t_tr
+            nets[p.method], train_rep[p.method] = net, rep
+            log(f"[bench] proposal for method {p.method} trained in {rep['wall_s']:.1f}s ({rep['labelled']} windows, "
+                f"holdout position median {rep['holdout_pos_median_px']:.3f} px)")
+    arm_opts = {"plain": lambda m: L.default_options(max_half_width=mh, precision=args.precision)}
+    if not args.no_warm:
+        arm_opts["warm"] = lambda m: L.default_options(max_half_width=mh, precision=args.precision,
+                                                       proposal=nets[m].handle.value)
+    if args.config == 3 and args.precision == 0:
+        arm_opts["fp64"] = lambda m: L.default_options(max_half_width=mh, precision=1)
+    opts = {arm: {p.method: f(p.method) for p in parts} for arm, f in arm_opts.items()}
 
     def step(arm):
-        o, f = outs[arm]
-        eng.fit_device(frames_dev.data_ptr(), n_frames, size, size, d_cands.data_ptr(), n, METHOD, w.w0, 1.0,
-                       o.data_ptr(), f.data_ptr(), stream.cuda_stream, arms[arm])
+        for p in parts:
+            o, f = p.out(torch, arm)
+            p.eng.fit_device(frames_dev.data_ptr(), n_frames, size, size, p.d_cands.data_ptr(), p.n, p.method, w.w0,
+                             1.0, o.data_ptr(), f.data_ptr(), stream.cuda_stream, opts[arm][p.method])
 
-    def timed(arm):
+    def timed(arm, steps):
         for _ in range(args.warmup):
             step(arm)
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
-        stage, stats_last = [], None
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with ClockSampler(local) as clk:
             torch.cuda.synchronize()
             start.record(stream)
-            for _ in range(args.steps):
+            for _ in range(steps):
                 step(arm)
-                # per-stage device times of this step (events on the same stream)
-                stats_last = eng.stats()
-                stage.append((stats_last["solver_ms"], stats_last["proposal_ms"]))
             end.record(stream)
             torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
         # whole-job throughput: summed work over the slowest rank's time
-        total, ms, rate = DI.job_throughput(n * args.steps, start.elapsed_time(end))
-        return {"value": rate, "ms": ms, "stats": stats_last, "clocks": clk.summary(),
-                "solver_ms": float(np.mean([a for a, _ in stage])), "proposal_ms": float(np.mean([b for _, b in stage]))}
+        total, ms, rate = DI.job_throughput(n * steps, start.elapsed_time(end))
+        # counters and stage times of the last step, per method
+        stats = {p.method: p.eng.stats() for p in parts}
+        return {"value": rate, "ms": ms, "stats": stats, "clocks": clk.summary(),
+                "solver_ms": float(sum(s["solver_ms"] for s in stats.values())),
+                "proposal_ms": float(sum(max(s["proposal_ms"], 0.0) for s in stats.values()))}
 
-    res = {arm: timed(arm) for arm in ("plain", "warm")}
+    res = {}
+    for arm in opts:
+        res[arm] = timed(arm, args.steps if arm != "fp64" else max(3, args.steps // 4))
+        log(f"[bench] arm {arm}: {res[arm]['value'] / 1e6:.2f} M fits/s, {res[arm]['ms'] / args.steps:.1f} ms/step")
     value = res["plain"]["value"]
     elapsed_ms = res["plain"]["ms"]
 
     # roofline of the plain solver: algorithmic FLOPs / solver time vs FP32 peak
     st = res["plain"]["stats"]
-    clocks = res["plain"]["clocks"]
-    p = NPAR[METHOD]
-    flops = st["pixels_j"] * FLOP_J[METHOD] + st["pixels_f"] * FLOP_F + st["lambda_solves"] * (p ** 3 / 3 + 2 * p * p)
+    flops = 0.0
+    for m, s in st.items():
+        pp = NPAR[m]
+        flops += s["pixels_j"] * FLOP_J[m] + s["pixels_f"] * FLOP_F + s["lambda_solves"] * (pp ** 3 / 3 + 2 * pp * pp)
     k_ms = res["plain"]["solver_ms"]
     achieved = flops / (k_ms / 1e3) / 1e12
-    peak_mhz = res["plain"]["clocks"]["sm_max_mhz"] or 1965.0
+    clocks = res["plain"]["clocks"]
+    peak_mhz = clocks["sm_max_mhz"] or 1965.0
     peak = SM_COUNT * FP32_LANES * 2 * peak_mhz * 1e6 / 1e12
-    # proposal network: algorithmic tensor-core FLOPs (valid conv2 + conv3
-    # outputs) per window over its device time vs the measured BF16 peak
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-    bf16_peak = peaks.get("bf16_tflops", 1590.0)
-    prop_ms = res["warm"]["proposal_ms"]
-    tc_flops = n * 2.0 * (49 * 144 * 32 + 25 * 288 * 32)
-    prop_roof = {"bound": "tensor", "kernel": "k_prop_fwd", "achieved": tc_flops / (prop_ms / 1e3) / 1e12,
-                 "peak": bf16_peak, "unit": "TFLOP/s", "frac": tc_flops / (prop_ms / 1e3) / 1e12 / bf16_peak,
-                 "kernel_ms": prop_ms, "windows_per_s": n / (prop_ms / 1e3),
-                 "peak_source": "bf16_tflops of measured MEASURED_PEAKS.json" if peaks else "fallback 1.59 PFLOP/s"}
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
+    prop_roof = None
+    if "warm" in res:
+        bf16_peak = peaks.get("bf16_tflops", 1590.0)
+        prop_ms = res["warm"]["proposal_ms"]
+        tc_flops = n * 2.0 * (49 * 144 * 32 + 25 * 288 * 32)
+        prop_roof = {"bound": "tensor", "kernel": "k_prop_fwd", "achieved": tc_flops / (prop_ms / 1e3) / 1e12,
+                     "peak": bf16_peak, "unit": "TFLOP/s", "frac": tc_flops / (prop_ms / 1e3) / 1e12 / bf16_peak,
+                     "kernel_ms": prop_ms, "windows_per_s": n / (prop_ms / 1e3),
+                     "peak_source": "bf16_tflops of measured MEASURED_PEAKS.json" if peaks else "fallback 1.59 PFLOP/s"}
 
-    # e2e through the host-buffer C ABI call (pinned host memory), warm-start arm
-    import ctypes as C
-    lib = L.lib()
-    ph_frames = torch.empty(frames_host.shape, dtype=torch.int16, pin_memory=True)
-    ph_frames.numpy().view(np.uint16)[...] = frames_host
-    ph_cands = torch.empty(cands.nbytes, dtype=torch.uint8, pin_memory=True)
-    ph_cands.numpy()[...] = cands.view(np.uint8)
-    ph_out = torch.empty((n, ncol), dtype=torch.float64, pin_memory=True)
-    ph_flags = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    # e2e through the host-buffer C ABI (pinned host memory), plain arm: one
+    # loc_fit_host_async call per block of frames (the whole stack for
+    # one-method configurations), closed by loc_fit_host_wait
+    e2e = None
+    frames_pinned = torch.empty(frames_dev.shape, dtype=torch.int16, pin_memory=True)
+    frames_pinned.copy_(frames_dev)
+    frames_host = frames_pinned.numpy().view(np.uint16)
+    if not args.no_e2e:
+        import ctypes as C
+        lib = L.lib()
+        blk = block if block > 0 else n_frames
+        chunks = []
+        fr_all = cands["frame"]
+        for b0 in range(0, n_frames, blk):
+            b1 = min(n_frames, b0 + blk)
+            lo, hi = np.searchsorted(fr_all, b0), np.searchsorted(fr_all, b1)
+            sub = cands[lo:hi].copy()
+            sub["frame"] -= b0
+            m = int(method_of(w, block, np.array([b0]))[0])
+            pc = torch.empty(sub.nbytes, dtype=torch.uint8, pin_memory=True)
+            pc.numpy()[...] = sub.view(np.uint8)
+            ncol = lib.loc_output_columns(m)
+            po = torch.empty((hi - lo, ncol), dtype=torch.float64, pin_memory=True)
+            pf = torch.empty(hi - lo, dtype=torch.uint8, pin_memory=True)
+            chunks.append((b0, b1, lo, hi, m, pc, po, pf))
+        assert np.all(np.diff(fr_all) >= 0)
+        e_eng = parts[0].eng
+        e_opts = {p.method: L.default_options(max_half_width=mh, precision=args.precision) for p in parts}
+        fb = frames_pinned.element_size() * size * size
 
-    def e2e_call(fn):
-        rc = fn(eng.handle, C.c_void_p(ph_frames.data_ptr()), n_frames, size, size,
-                C.c_void_p(ph_cands.data_ptr()), n, METHOD, w.w0, 1.0, C.byref(arms["plain"]),
-                C.c_void_p(ph_out.data_ptr()), C.c_void_p(ph_flags.data_ptr()))
-        if rc != 0:
-            raise RuntimeError(lib.loc_last_error().decode())
+        def e2e_step():
+            for b0, b1, lo, hi, m, pc, po, pf in chunks:
+                rc = lib.loc_fit_host_async(e_eng.handle, C.c_void_p(frames_pinned.data_ptr() + b0 * fb), b1 - b0,
+                                            size, size, C.c_void_p(pc.data_ptr()), hi - lo, m, w.w0, 1.0,
+                                            C.byref(e_opts[m]), C.c_void_p(po.data_ptr()), C.c_void_p(pf.data_ptr()))
+                if rc != 0:
+                    raise RuntimeError(lib.loc_last_error().decode())
 
-    def e2e_rate(streamed: bool) -> float:
-        """Whole-job fits/s of e2e_steps host-buffer calls: one loc_fit_host
-        per step, or a stream of loc_fit_host_async calls (each step's upload
-        overlapping the previous step's fit) closed by loc_fit_host_wait."""
-        fn = lib.loc_fit_host_async if streamed else lib.loc_fit_host
-        for _ in range(2):
-            e2e_call(fn)
-        if lib.loc_fit_host_wait(eng.handle) != 0:
-            raise RuntimeError(lib.loc_last_error().decode())
+        def wait():
+            if lib.loc_fit_host_wait(e_eng.handle) != 0:
+                raise RuntimeError(lib.loc_last_error().decode())
+
+        e_steps = args.e2e_steps or min(args.steps, 10)
+        e2e_step()
+        wait()
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
         dstream = torch.cuda.default_stream()
         s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s2.record(dstream)
-        for _ in range(args.e2e_steps):
-            e2e_call(fn)
-        if lib.loc_fit_host_wait(eng.handle) != 0:
-            raise RuntimeError(lib.loc_last_error().decode())
+        for _ in range(e_steps):
+            e2e_step()
+        wait()
         e2.record(dstream)
         torch.cuda.synchronize()
-        t2 = torch.tensor([s2.elapsed_time(e2) / args.e2e_steps], device="cuda")
-        if world > 1:
-            torch.distributed.all_reduce(t2, op=torch.distributed.ReduceOp.MAX)
-        return value * elapsed_ms / 1e3 / args.steps / (t2.item() / 1e3)
+        _, e_ms, e_rate = DI.job_throughput(n * e_steps, s2.elapsed_time(e2))
+        e2e = {"value": e_rate, "unit": UNIT, "h2d_bytes_per_step": int(frames_dev.numel() * 2 + cands.nbytes),
+               "d2h_bytes_per_step": int(sum(po.numel() * 8 + pf.numel() for *_, po, pf in chunks)), "arm": "plain",
+               "call": f"loc_fit_host_async per block of {blk} frames ({len(chunks)} calls per step, pinned host "
+                       f"buffers, uploads overlapping the previous call's fit), loc_fit_host_wait at the end",
+               "steps": e_steps, "ms_per_step": e_ms / e_steps}
+        # the host-buffer path gives the device path's rows
+        for b0, b1, lo, hi, m, pc, po, pf in chunks:
+            p = next(q for q in parts if q.method == m)
+            pos = np.searchsorted(p.idx, np.arange(lo, hi))
+            o, f = p.out(torch, "plain")
+            sel = torch.from_numpy(pos).cuda()
+            assert np.array_equal(pf.numpy(), f[sel].cpu().numpy())
+            assert np.array_equal(po.numpy()[:, :-2], o[sel].cpu().numpy()[:, :-2], equal_nan=True)
+        log(f"[bench] e2e: {e_rate / 1e6:.2f} M fits/s")
 
-    e2e_sync = e2e_rate(False)
-    e2e = {"value": e2e_rate(True), "unit": UNIT,
-           "h2d_bytes_per_step": int(frames_host.nbytes + cands.nbytes),
-           "d2h_bytes_per_step": int(n * ncol * 8 + n), "arm": "plain",
-           "call": "loc_fit_host_async per step (pinned host buffers; a step's upload overlaps the previous step's "
-                   "fit), loc_fit_host_wait at the end", "steps": args.e2e_steps,
-           "one_call_per_step_value": e2e_sync}
-    rows_e2e = ph_out.numpy().copy()
-    flags_e2e = ph_flags.numpy().copy()
-
-    # CPU reference on a bounded sample, and the accuracy of both arms there
+    # CPU reference on a bounded sample of whole frames, and the accuracy of
+    # every arm there
     cpu, accuracy = None, None
     if rank == 0 and not args.no_cpu_baseline:
         from oracle import oracle as O
-        rows = {k: outs[k][0].cpu().numpy() for k in outs}
-        flg = {k: outs[k][1].cpu().numpy() for k in outs}
-        assert np.array_equal(rows["plain"][:, :ncol - 2], rows_e2e[:, :ncol - 2], equal_nan=True)
-        assert np.array_equal(flg["plain"], flags_e2e)
         if O.ref_available():
-            v, ns, th, idx, rrows, rkept = run_reference_sample(frames_host, cands, w.w0, budget_s=args.ref_budget)
-            cpu = {"value": v, "unit": UNIT, "cores": th, "kind": "reference",
-                   "sample": f"{ns} candidates (whole frames spread through the stack); reference "
-                             f"Localization.cpp FP64 + lmsder restatement, {th} host threads"}
-            accuracy = {"sample_fits": int(len(idx)), "reference": "reference fitter (FP64) on the same candidates"}
-            for k in ("plain", "warm"):
-                g = rows[k][idx]
-                gk = flg[k][idx] == 0
-                both = gk & rkept
-                err = np.abs(g[both, 4:6] - rrows[both, 4:6]).max(axis=1)
-                accuracy[k] = {"flag_agreement": float(np.mean(gk == rkept)),
-                               "position_within_1e-3px": float(np.mean(err < 1e-3)) if len(err) else None,
-                               "position_max_err_px": float(err.max()) if len(err) else None}
+            threads = os.cpu_count() or 1
+            per_fit = calibrate_per_fit(frames_host, cands, methods, w.w0)
+            chosen = sample_frames(n_frames, n / n_frames, args.ref_budget_repo * threads / per_fit, threads)
+            sel = np.nonzero(np.isin(cands["frame"], chosen))[0]
+            dt, ref, th = ref_fit_parallel(frames_host, cands[sel], methods[sel], w.w0, threads)
+            cpu = {"value": len(sel) / dt, "unit": UNIT, "cores": th, "kind": "reference",
+                   "sample": f"{len(sel)} candidates of {len(chosen)} whole frames spread through the stack; "
+                             f"reference Localization.cpp FP64 + lmsder restatement, {th} host threads"}
+            accuracy = {"sample_fits": int(len(sel)), "reference": "reference fitter (FP64) on the same candidates"}
+            for arm in res:
+                accuracy[arm] = {}
+                for p in parts:
+                    idx_s, rrows, rkept, rit = ref[p.method]
+                    gidx = sel[idx_s]                     # global candidate index
+                    pos = np.searchsorted(p.idx, gidx)    # row in the part
+                    o, f = p.out(torch, arm)
+                    t = torch.from_numpy(pos).cuda()
+                    accuracy[arm][f"method_{p.method}"] = accuracy_report(o[t].cpu().numpy(), f[t].cpu().numpy(),
+                                                                          rrows, rkept, rit, p.method)
 
     next_rows = None
+    if rank == 0 and not args.no_next_rows:
+        p = parts[-1]
+        o, f = p.out(torch, "plain")
+        next_rows = measure_next_rows(L, torch, p.eng, frames_dev, frames_host, p, w.w0, o.cpu().numpy(),
+                                      f.cpu().numpy(), peaks.get("hbm_gbs", 6650.0), peaks)
     if rank == 0:
-        next_rows = measure_next_rows(eng, frames_dev, frames_host, cands, d_cands, w.w0,
-                                      outs["plain"][0].cpu().numpy(), outs["plain"][1].cpu().numpy(),
-                                      peaks.get("hbm_gbs", 6650.0))
-    if rank == 0:
-        sw = res["warm"]["stats"]
+        launches = sum(int(s["kernel_launches"]) for s in st.values())
+        per_method = {m: {"fits": int(s["fits"]), "iterations_per_fit": s["iterations"] / max(s["fits"], 1),
+                          "fits_fp64_rerun": int(s["fits_fp64_rerun"]),
+                          "fp64_rerun_fraction": s["fits_fp64_rerun"] / max(s["fits"], 1),
+                          "solver_ms": s["solver_ms"]} for m, s in st.items()}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == 0 else "f64",
                 "data": "synthetic (seeded emitters, GPU-rendered Poisson+read-noise frames)",
-                "config": {"workload": "batched uneven: 10000 frames 256x256 uint16, 20-400 emitters/frame, "
-                                       "ellipsoidal PSF sigma U[1,2], ROI half-width in {3,4,5,6}, method 7",
-                           "frames_per_gpu": n_frames, "candidates_per_gpu": n, "parallelism": f"dp{world}",
-                           "l2": "inputs larger than L2 (1.3 GB frames, 71 MB candidates, 256 MB rows)"},
-                "warm_start_lm_fits_per_s": res["warm"]["value"], "plain_lm_fits_per_s": value,
-                "warm_vs_plain": res["warm"]["value"] / value,
-                "warm_ms_per_step": res["warm"]["ms"] / args.steps, "value_arm": "plain",
-                "warm_start": {"fits_warm": sw["fits_warm"], "fits_cold_fallback": sw["fits_fp64_rerun"],
-                               "iterations_per_fit": sw["iterations"] / max(sw["fits"], 1),
-                               "plain_iterations_per_fit": st["iterations"] / max(st["fits"], 1),
-                               "proposal_ms": prop_ms, "solver_ms": res["warm"]["solver_ms"],
-                               "training": train_rep},
+                "config": {"workload": CONFIGS[args.config]["label"], "config": args.config,
+                           "frames_per_gpu": n_frames, "candidates_per_gpu": n,
+                           "methods": {str(p.method): p.n for p in parts}, "parallelism": f"dp{world}",
+                           "l2": f"inputs larger than L2 ({frames_dev.numel() * 2 / 1e9:.2f} GB frames)"},
+                "value_arm": "plain", "plain_lm_fits_per_s": value,
+                "plain": {"per_method": per_method, "solver_ms": k_ms},
                 "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                             "frac": achieved / peak, "traffic": 304.0 * n,
-                             "traffic_note": "DRAM bytes per step of the level-0 FP32 solver, scaled from the "
-                                             "ncu capture of 1000 frames (r = 6 class: 13.4 MB read, 0 written "
-                                             "for about 44 k fits = 304 B per fit; ROI gather of 338 B per "
-                                             "13 x 13 ROI, partly from L2)",
+                             "frac": achieved / peak,
+                             "traffic": TRAFFIC_PER_FIT["bytes"] * n if TRAFFIC_PER_FIT else None,
+                             "traffic_note": (f"DRAM bytes per step of the plain solver chain, "
+                                              f"{TRAFFIC_PER_FIT['bytes']:.0f} B per fit from "
+                                              f"{TRAFFIC_PER_FIT['source']}") if TRAFFIC_PER_FIT else
+                             "no ncu capture of the current solver chain",
                              "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 x max SM clock); "
                                             "no measured FP32 peak in MEASURED_PEAKS.json",
-                             "kernel": "k1_lm_fit (plain arm, all classes and levels)", "kernel_ms": k_ms,
-                             "flops_per_step": flops},
-                "proposal_roofline": prop_roof, "finder": finder,
-                "stats": st, "warm_stats": sw, "clocks": clocks, "warm_clocks": res["warm"]["clocks"], "e2e": e2e, "cpu_baseline": cpu,
-                "accuracy": accuracy, "next_rows": next_rows,
-                "gpu_launches": int(st["kernel_launches"]) * args.steps}
+                             "kernel": "k1_lm_fit + k3_flag_class + k2_finalize (plain arm, every ROI class and "
+                                       "level)", "kernel_ms": k_ms, "flops_per_step": flops},
+                "finder": finder, "stats": st, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
+                "accuracy": accuracy, "next_rows": next_rows, "gpu_launches": launches * args.steps}
+        if "warm" in res:
+            sw = res["warm"]["stats"]
+            line.update({"warm_start_lm_fits_per_s": res["warm"]["value"],
+                         "warm_vs_plain": res["warm"]["value"] / value,
+                         "warm_ms_per_step": res["warm"]["ms"] / args.steps,
+                         "warm_start": {"per_method": {m: {
+                             "fits_warm": int(s["fits_warm"]), "fits_cold_fallback": int(s["fits_fp64_rerun"]),
+                             "iterations_per_fit": s["iterations"] / max(s["fits"], 1),
+                             "plain_iterations_per_fit": st[m]["iterations"] / max(st[m]["fits"], 1)}
+                             for m, s in sw.items()},
+                             "proposal_ms": res["warm"]["proposal_ms"], "solver_ms": res["warm"]["solver_ms"],
+                             "training": train_rep},
+                         "proposal_roofline": prop_roof, "warm_clocks": res["warm"]["clocks"]})
+        if "fp64" in res:
+            line["precision_report"] = precision_report(res, accuracy, parts)
         print(json.dumps(line))
-    net.close()
-    eng.close()
+    for net in nets.values():
+        net.close()
+    for p in parts:
+        p.eng.close()
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def precision_report(res, accuracy, parts):
+    """The precision-stress comparison: the FP32 solver (compensated by its
+    FP64 re-run of decision-sensitive fits) against the GPU FP64 solver and
+    the CPU FP64 reference."""
+    rep = {}
+    for arm in ("plain", "fp64"):
+        s = res[arm]["stats"]
+        rep[arm] = {"fits_per_s": res[arm]["value"],
+                    "fits_fp64_rerun": int(sum(v["fits_fp64_rerun"] for v in s.values())),
+                    "fp64_rerun_fraction": sum(v["fits_fp64_rerun"] for v in s.values()) /
+                    max(sum(v["fits"] for v in s.values()), 1),
+                    "fp64_pivot_escalations": int(sum(v["fp64_escalations"] for v in s.values())),
+                    "vs_cpu_reference": accuracy.get(arm) if accuracy else None}
+    return rep
+
+
+def measure_next_rows(L, torch, eng, frames_dev, frames_host, part, w0, rows_plain, flags_plain, hbm_peak, peaks):
+    """Throughput of the path's neighbours on the same workload, outside the
+    timed region: frame ingest (row-major float32 camera frames -> the
+    uint16 stack, HBM-bound at 4 + 2 B per pixel), the MLEwG fit (method 6)
+    against the reference's own MLEwG on one host core, and the positions
+    text writer."""
+    import tempfile
+
+    from oracle import oracle as O
+    out = {}
+    nf = max(1, min(frames_dev.shape[0], (2000 * 256 * 256) // (frames_dev.shape[1] * frames_dev.shape[2])))
+    src = (frames_dev[:nf].to(torch.int32) & 0xFFFF).to(torch.float32).transpose(1, 2).contiguous()
+    dst, lossy = L.ingest_frames(src, row_major=True)
+    assert lossy == 0 and torch.equal(dst, frames_dev[:nf])
+    reps = 10
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        L.ingest_frames(src, row_major=True)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    gbs = src.numel() * 6 / (ms / 1e3) / 1e9
+    out["ingest"] = {"kernel": "k_ingest_rm<float>", "frames": nf, "ms_per_call": ms, "frames_per_s": nf / (ms / 1e3),
+                     "achieved_gbs": gbs, "peak_gbs": hbm_peak, "frac": gbs / hbm_peak,
+                     "bytes_per_pixel": 6, "check": "lossless round trip of the uint16 stack",
+                     "timing": "per call, including the call's host synchronisation for the lossy count",
+                     "peak_source": "hbm_gbs of measured MEASURED_PEAKS.json" if peaks else "fallback 6.65 TB/s"}
+    del src, dst
+    k = min(100000, part.n)
+    ncol6 = L.lib().loc_output_columns(6)
+    o6 = torch.empty((k, ncol6), dtype=torch.float64, device="cuda")
+    f6 = torch.empty(k, dtype=torch.uint8, device="cuda")
+    opt6 = L.default_options(max_half_width=int(part.cands["half_width"].max()))
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def fit6():
+        eng.fit_device(frames_dev.data_ptr(), frames_dev.shape[0], frames_dev.shape[2], frames_dev.shape[1],
+                       part.d_cands.data_ptr(), k, 6, w0, 1.0, o6.data_ptr(), f6.data_ptr(), stream, opt6)
+
+    fit6()
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(3):
+        fit6()
+    b.record()
+    torch.cuda.synchronize()
+    ms6 = a.elapsed_time(b) / 3
+    mlewg = {"candidates": k, "ms_per_call": ms6, "fits_per_s": k / (ms6 / 1e3)}
+    if O.ref_available():
+        f0 = int(part.cands["frame"][0])
+        sel = np.nonzero(part.cands["frame"][:k] == f0)[0]
+        t = time.perf_counter()
+        rout, rkept, _, _ = O.ref_fit(frames_host, np.ascontiguousarray(part.cands[sel]), 6, w0)
+        dt = time.perf_counter() - t
+        g = o6[torch.from_numpy(sel).cuda()].cpu().numpy()
+        gk = f6[torch.from_numpy(sel).cuda()].cpu().numpy() == 0
+        rk = rkept == 1
+        same = (gk == rk) & (~gk | np.all(g[:, :8] == rout[:, :8], axis=1))
+        mlewg["reference_one_core"] = {"fits_per_s": len(sel) / dt, "fits": int(len(sel)),
+                                       "sample": f"the {len(sel)} candidates of frame {f0}"}
+        mlewg["identical_to_reference"] = float(np.mean(same))
+    out["mlewg"] = mlewg
+    m = min(300000, len(rows_plain))
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "positions.txt")
+        t = time.perf_counter()
+        kept = L.write_positions(path, rows_plain[:m], flags_plain[:m], part.method, "bench")
+        dt = time.perf_counter() - t
+        size = os.path.getsize(path)
+    out["writer"] = {"rows": m, "kept_rows_written": int(kept), "s": dt, "rows_per_s": m / dt,
+                     "mb_per_s": size / dt / 1e6, "threads": os.cpu_count()}
+    return out
 
 
 if __name__ == "__main__":

@@ -238,18 +238,21 @@ LOC_API int loc_fit_host_wait(loc_ctx *ctx);
 
 /*
  * Allocation-free form of loc_fit_batch (same arguments, no context, same
- * results). It has no counterpart in the reference, which fits on the CPU
- * and allocates freely; it exists for callers that may not allocate device
- * memory: code running under a framework whose caching allocator owns the
- * device heap, plugins handed only their input and output buffers, and
- * acquisition loops that must not call cudaMalloc/cudaFree between frames.
- * All device scratch comes from one file-scope device array of 16 MiB,
- * reserved on each GPU where this entry point is used until the process
- * exits. At most 16384 candidates per call (larger calls fail with
- * LOC_E_UNSUPPORTED before any device work). Calls share the array: the call
- * resets what must start at zero, but calls that overlap on the GPU race and
- * must be serialised. The first call on a device resolves the array's
- * address; make it before any stream capture. Errors: negative LOC_E_* code,
+ * results for methods 0, 1, 5 and 7; method 6 and start proposals are
+ * refused with LOC_E_UNSUPPORTED). It has no counterpart in the reference,
+ * which fits on the CPU and allocates freely; it exists for callers that may
+ * not allocate device memory: code running under a framework whose caching
+ * allocator owns the device heap, plugins handed only their input and output
+ * buffers, and acquisition loops that must not call cudaMalloc/cudaFree
+ * between frames. All device scratch comes from one file-scope device array
+ * of 16 MiB, reserved until the process exits on each GPU where the
+ * library's device code is loaded (with CUDA's default lazy module loading:
+ * where this entry point is used). At most 16384 candidates per call (larger
+ * calls fail with LOC_E_UNSUPPORTED before any device work). Calls share the
+ * array: the call resets what must start at zero, but calls that overlap on
+ * the GPU race and must be serialised. The first call on a device resolves
+ * the array's address; make it before any stream capture, and make no call
+ * on a device after a cudaDeviceReset of it. Errors: negative LOC_E_* code,
  * message through loc_last_error().
  */
 LOC_API int loc_fit_batch_static(const uint16_t *d_frames, int n_frames, int n_rows, int n_cols,

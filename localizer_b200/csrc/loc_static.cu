@@ -14,8 +14,14 @@
 // Limits and sharing rules:
 //  - at most kStaticMaxCands candidates per call (16384); larger calls are
 //    rejected with LOC_E_UNSUPPORTED before any device work;
-//  - the array (kStaticScratchBytes, 16 MiB) is reserved on every GPU on which
-//    this entry point has been called, until the process exits;
+//  - the array (kStaticScratchBytes, 16 MiB) is reserved, until the process
+//    exits, on every GPU where the library's device code is loaded: with
+//    lazy module loading (CUDA's default, CUDA_MODULE_LOADING=LAZY) that is
+//    the GPUs on which this entry point has been called, with
+//    CUDA_MODULE_LOADING=EAGER every GPU whose context loads the library;
+//  - method 6 (MLEwG) and start proposals are not available here (they
+//    need a context); every other method and option gives loc_fit_batch's
+//    results;
 //  - every call on a device uses the same array and leaves its contents
 //    behind; the call clears what must start at zero (queue tables and
 //    counters) itself, so results never depend on a previous call, but two
@@ -46,6 +52,9 @@ constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
+// resolved once per device; the address does not survive cudaDeviceReset
+// (the module is loaded again and the array may move), so a process that
+// resets a device must not call this entry point on it afterwards
 void *g_scratch_ptr[kMaxDevices] = {};
 std::mutex g_setup_mu;
 

@@ -213,13 +213,14 @@ def frame_labels(frames, cands: np.ndarray, method: int, w0: float, engine: Engi
     return labels, valid
 
 
-def workload_windows(n_frames: int, method: int, seed: int, pfa: float = 30.0):
-    """Windows cut from synthetic frames of the batched uneven workload type
-    (seeded, disjoint from the evaluation seeds), labelled by the plain LM
-    fit of their candidates at the candidates' own ROI half-widths."""
+def workload_windows(n_frames: int, method: int, seed: int, pfa: float = 30.0, workload: str = "uneven"):
+    """Windows cut from synthetic frames of a workload type (the batched
+    uneven one by default; seeded, disjoint from the evaluation seeds),
+    labelled by the plain LM fit of their candidates at the candidates' own
+    ROI half-widths."""
     from . import find_candidates
     from . import synth
-    w = synth.scaled(synth.workloads()["uneven"], n_frames, seed=seed)
+    w = synth.scaled(synth.workloads()[workload], n_frames, seed=seed)
     frames, _ = synth.make_device(w)
     host = frames.cpu().numpy().view(np.uint16)
     cands = find_candidates(host, pfa, w.w0)
@@ -262,11 +263,12 @@ def to_params(out: np.ndarray, b0: np.ndarray, s0: np.ndarray, nout: int) -> np.
 
 
 def train(method: int = 7, n_rois: int = 2_000_000, epochs: int = 8, batch: int = 4096, lr: float = 2e-3,
-          seed: int = 7, device: int = 0, holdout: float = 0.02, log=None, frames: int = 0):
+          seed: int = 7, device: int = 0, holdout: float = 0.02, log=None, frames: int = 0,
+          workload: str = "uneven"):
     """Generate, label and train. Windows: n_rois isolated synthetic windows
     (loc_synth_rois), plus, if frames > 0, the candidates' windows of that
-    many synthetic frames of the batched uneven workload. Returns
-    (Proposal, report dict)."""
+    many synthetic frames of the named workload type (the batched uneven one
+    by default). Returns (Proposal, report dict)."""
     import torch
     t0 = time.time()
     nout = NOUT[method]
@@ -276,7 +278,7 @@ def train(method: int = 7, n_rois: int = 2_000_000, epochs: int = 8, batch: int 
         lab, val = label_rois(r, method)
         parts_r.append(r); parts_l.append(lab); parts_v.append(val)
     if frames > 0:
-        r, lab, val = workload_windows(frames, method, seed=100_000 + seed)
+        r, lab, val = workload_windows(frames, method, seed=100_000 + seed, workload=workload)
         parts_r.append(r); parts_l.append(lab); parts_v.append(val)
     rois = torch.cat(parts_r) if len(parts_r) > 1 else parts_r[0]
     labels = torch.cat(parts_l) if len(parts_l) > 1 else parts_l[0]

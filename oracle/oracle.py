@@ -19,6 +19,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libloc_ref.so")
+CAPI_SO = os.path.join(HERE, "_ref", "libfitpositions_gpu.so")
 
 CAND_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("intensity", "<f8"), ("background", "<f8"),
                        ("frame", "<i4"), ("half_width", "<i4")], align=True)
@@ -37,13 +38,24 @@ _lib = None
 _ref = None
 
 
+# the reference tree the Makefile compiles from: $LOC_REFERENCE, else the
+# Makefile's own default (its REF variable)
+DEFAULT_REF = "/root/reference"
+
+
+def reference_tree() -> str:
+    return os.environ.get("LOC_REFERENCE", DEFAULT_REF)
+
+
 def build():
-    """Compile the oracle (and the reference build when the tree exists)."""
+    """Compile the oracle, and, when the reference tree exists, the reference
+    build and the C++ adapter test library (after the product library)."""
     import subprocess
+    ref = reference_tree()
     targets = ["oracle"]
-    if os.path.isdir("/root/reference/source"):
-        targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    if os.path.isdir(os.path.join(ref, "source")):
+        targets += ["ref", "capi"]
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={ref}"] + targets, check=True)
 
 
 def lib():
@@ -85,6 +97,11 @@ def ref():
                               C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.ref_find_adjacent8.restype = C.c_int
         L.ref_find_adjacent8.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+        L.ref_glrt_mask.restype = C.c_int
+        L.ref_glrt_mask.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p]
+        L.ref_find_candidates.restype = C.c_long
+        L.ref_find_candidates.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                          C.c_void_p, C.c_long]
         L.ref_write_positions.restype = C.c_int
         L.ref_write_positions.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                           C.c_double, C.c_double, C.c_char_p, C.c_char_p]
@@ -173,6 +190,63 @@ def _find(fn, frame2d, mask, max_out=1 << 16):
     return out[:min(n, max_out)].copy()
 
 
+def ref_glrt_mask(frame2d, pfa, psf_width):
+    """The reference's own ThresholdImage_GLRT_FFT mask (FFT correlation on
+    fftw_shim.c) of one frame [y, x]: 255 where detected."""
+    frame2d = np.ascontiguousarray(frame2d, dtype=np.uint16)
+    n_cols, n_rows = frame2d.shape
+    mask = np.zeros((n_cols, n_rows), dtype=np.int32)
+    if ref().ref_glrt_mask(frame2d.ctypes.data, n_rows, n_cols, pfa, psf_width, mask.ctypes.data) != 0:
+        raise RuntimeError("ref_glrt_mask failed")
+    return mask
+
+
+def ref_find_candidates(frames, pfa, psf_width):
+    """The reference's own candidate pipeline (GLRT + adjacent-8, one
+    thresholder and finder for the stack) as a CAND_DTYPE array in frame
+    order, half_width 0."""
+    n_frames, n_rows, n_cols = _stack_dims(frames)
+    cap = max(1024, 64 * n_frames)
+    while True:
+        out = np.zeros((cap, 5))
+        n = ref().ref_find_candidates(frames.ctypes.data, n_frames, n_rows, n_cols, pfa, psf_width,
+                                      out.ctypes.data, cap)
+        if n < 0:
+            raise RuntimeError("ref_find_candidates failed")
+        if n <= cap:
+            break
+        cap = n
+    c = np.zeros(n, dtype=CAND_DTYPE)
+    for k, name in enumerate(("x", "y", "intensity", "background")):
+        c[name] = out[:n, k]
+    c["frame"] = out[:n, 4].astype(np.int32)
+    return c
+
+
+def glrt_statistic(frame2d, psf_width, pixels):
+    """The GLRT test statistic (Segmentation.cpp:400-420) at the given
+    (x, y) pixels, by direct sums in FP64 (exact box sums)."""
+    f = np.asarray(frame2d, dtype=np.float64)
+    ws = int(np.ceil(4 * psf_width))
+    ws += 1 - ws % 2
+    half = ws // 2
+    npix = float(ws * ws)
+    d = np.arange(-half, half + 1, dtype=np.float64)
+    g = 1.0 / (1.77245385 * psf_width) * np.exp(-1.0 / (2.0 * psf_width * psf_width) *
+                                              (d[None, :] ** 2 + d[:, None] ** 2))
+    g = g - g.sum() / npix
+    sumsq = float((g * g).sum())
+    out = []
+    for x, y in pixels:
+        win = f[y - half:y + half + 1, x - half:x + half + 1]
+        s1, s2 = win.sum(), (win * win).sum()
+        avg = s1 / npix
+        null_h = s2 - avg * avg * npix
+        alpha = float((win * g).sum()) / sumsq
+        out.append(alpha * alpha / null_h * sumsq)
+    return np.array(out)
+
+
 def find_adjacent8(frame2d, mask):
     return _find(lib().oracle_find_adjacent8, frame2d, mask)
 
@@ -232,3 +306,38 @@ def ref_write_positions(frames, cands, method, w0, path, header="", sigma=1.0):
     if rc < 0:
         raise RuntimeError(f"ref_write_positions failed: {rc}")
     return rc
+
+
+def capi_available() -> bool:
+    return os.path.exists(CAPI_SO)
+
+
+def capi_compare(frames, cands, method, w0, sigma=1.0, device=0):
+    """Per-frame fit_positions calls of the C++ FitPositions_GPU adapter
+    (tests/capi/fitpositions_gpu.cpp, over the product's C ABI) and of the
+    reference's own fitter on the same particle lists, merged per side as
+    the reference's controller merges them. Returns a dict with both merged
+    matrices (N x C) and the (x, y) of the particles each side left in its
+    lists."""
+    L = C.CDLL(CAPI_SO)
+    fn = L.fpgpu_compare
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double,
+                   C.c_double, C.c_int, C.c_void_p, C.POINTER(C.c_int), C.c_void_p, C.POINTER(C.c_int), C.c_int,
+                   C.c_void_p, C.POINTER(C.c_int), C.c_void_p, C.POINTER(C.c_int)]
+    n_frames, n_rows, n_cols = _stack_dims(frames)
+    cands = np.ascontiguousarray(cands, dtype=CAND_DTYPE)
+    n = len(cands)
+    parts = np.ascontiguousarray(np.stack([cands["x"], cands["y"], cands["intensity"], cands["background"]], axis=1))
+    frame_of = np.ascontiguousarray(cands["frame"], dtype=np.int32)
+    ncol = REF_COLUMNS[method]
+    gm, rm = np.zeros((max(n, 1), ncol)), np.zeros((max(n, 1), ncol))
+    gl, rl = np.zeros((max(n, 1), 2)), np.zeros((max(n, 1), 2))
+    ng, nr, ngl, nrl = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    rc = fn(frames.ctypes.data, n_frames, n_rows, n_cols, parts.ctypes.data, frame_of.ctypes.data, n, method, w0,
+            sigma, device, gm.ctypes.data, C.byref(ng), rm.ctypes.data, C.byref(nr), max(n, 1), gl.ctypes.data,
+            C.byref(ngl), rl.ctypes.data, C.byref(nrl))
+    if rc != 0:
+        raise RuntimeError("fpgpu_compare failed")
+    return {"gpu_matrix": gm[:ng.value], "ref_matrix": rm[:nr.value], "gpu_left": gl[:ngl.value],
+            "ref_left": rl[:nrl.value]}

@@ -263,6 +263,57 @@ int ref_write_positions(const uint16_t *frames, int n_frames, int n_rows, int n_
     }
 }
 
+/* The reference's own GLRT detector (ThresholdImage_GLRT_FFT,
+ * Segmentation.cpp:241-430, with its FFT-based Gaussian correlation running
+ * on fftw_shim.c) on one frame: mask_out receives 255 / 0 per pixel,
+ * column-major like the frame. */
+int ref_glrt_mask(const uint16_t *frame, int n_rows, int n_cols, double pfa, double psf_width, int32_t *mask_out)
+{
+    try {
+        ImagePtr img = frame_image(frame, 0, n_rows, n_cols);
+        ThresholdImage_GLRT_FFT th(pfa, psf_width);
+        auto m = th.do_thresholding(img);
+        for (int j = 0; j < n_cols; j++)
+            for (int i = 0; i < n_rows; i++) mask_out[i + (size_t)j * n_rows] = (*m)(i, j);
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+/* The reference's candidate pipeline over a stack, as its analysis
+ * controller runs it per frame (PALMAnalysis.cpp:214-227, one thresholder
+ * and one finder for the whole stack): GLRT + adjacent-8. out receives
+ * (x, y, intensity, background, frame) per particle in frame order; returns
+ * the number found (only max_out are written) or -1. */
+long ref_find_candidates(const uint16_t *frames, int n_frames, int n_rows, int n_cols, double pfa,
+                         double psf_width, double *out, long max_out)
+{
+    try {
+        ThresholdImage_GLRT_FFT th(pfa, psf_width);
+        ParticleFinder_adjacent8 finder;
+        long k = 0;
+        for (int f = 0; f < n_frames; f++) {
+            ImagePtr img = frame_image(frames, f, n_rows, n_cols);
+            auto m = th.do_thresholding(img);
+            auto parts = finder.findPositions(img, m);
+            for (auto &p : *parts) {
+                if (k < max_out) {
+                    out[5 * k + 0] = p.x;
+                    out[5 * k + 1] = p.y;
+                    out[5 * k + 2] = p.intensity;
+                    out[5 * k + 3] = p.background;
+                    out[5 * k + 4] = (double)f;
+                }
+                k++;
+            }
+        }
+        return k;
+    } catch (...) {
+        return -1;
+    }
+}
+
 /* The reference's adjacent-8 finder on a given mask (255 = detected). */
 int ref_find_adjacent8(const uint16_t *frame, int n_rows, int n_cols, const int32_t *mask,
                        double *out, int max_out)

@@ -71,6 +71,39 @@ def test_static_entry_matches_batched_fit_twice():
         eng.close()
 
 
+def test_static_entry_allocates_no_device_memory():
+    """After the first call on the device (which resolves the array's
+    address), a call leaves the device's free memory unchanged: its scratch
+    is the static array, not an allocation. No context is alive here."""
+    import torch
+    lib = L.lib()
+    g, frames, cands, d_frames, d_cands = _inputs("uneven")
+    n = len(cands)
+    n_frames, n_cols, n_rows = frames.shape
+    out, flags = _outputs(n, 7)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def call():
+        rc = lib.loc_fit_batch_static(C.c_void_p(d_frames.data_ptr()), n_frames, n_rows, n_cols,
+                                      C.c_void_p(d_cands.data_ptr()), n, 7, g["w0"], 1.0, None,
+                                      C.c_void_p(out.data_ptr()), C.c_void_p(flags.data_ptr()), C.c_void_p(stream))
+        assert rc == 0, lib.loc_last_error()
+        torch.cuda.synchronize()
+
+    call()
+    free0 = torch.cuda.mem_get_info()[0]
+    call()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free1 == free0, (free0, free1)
+    assert np.sum(flags.cpu().numpy() == 0) > 0.5 * n
+
+
+def test_static_entry_refuses_unsupported_modes():
+    lib = L.lib()
+    rc = lib.loc_fit_batch_static(None, 1, 64, 64, None, 0, 6, 1.3, 1.0, None, None, None, None)
+    assert rc == -4
+
+
 def test_static_entry_refuses_oversized_batch():
     lib = L.lib()
     rc = lib.loc_fit_batch_static(None, 1, 64, 64, None, 16385, 0, 1.3, 1.0, None, None, None, None)
