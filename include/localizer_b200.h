@@ -161,6 +161,20 @@ typedef struct loc_options {
                                   more solver iterations than this are re-run
                                   from the reference start (in FP64, the
                                   reference's algorithm); 0: default 8, < 0: never */
+    int32_t long_rerun_iters;  /* FP64 re-runs of fits whose FP32 solve took more
+                                  iterations than this form their own queue,
+                                  solved with long_rerun_threads_per_fit threads
+                                  per fit on a second stream of their chain (they
+                                  set the length of the re-run); 0: default, the
+                                  level-0 budget; < 0: one queue */
+    int32_t long_rerun_threads_per_fit; /* 1, 2, 4 or 8; 0: default 8 */
+    int32_t compensated;       /* 1: two-level summation of the FP32 normal
+                                  equations: each of a fit's threads sums its
+                                  share of the ROI pixels in FP32 and the
+                                  partial sums are combined in FP64 and rounded
+                                  once (the first scheduling level then runs at
+                                  least 4 threads per fit); 0 (default): FP32
+                                  throughout */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */
@@ -259,6 +273,39 @@ LOC_API int loc_fit_batch_static(const uint16_t *d_frames, int n_frames, int n_r
                                  const loc_candidate *d_cands, int n_cands, int method, double w0,
                                  double sigma, const loc_options *opt, double *d_out, uint8_t *d_flags,
                                  void *stream);
+
+/*
+ * Launch-shape tuner (no reference counterpart: the reference's fit is a
+ * serial CPU loop). Times the FP32 solver on a caller-supplied sample of
+ * candidates (device buffers, as for loc_fit_batch; a few 10^4 to 10^5
+ * candidates of the workload to be fitted) over its launch shapes -- threads
+ * per block, threads per fit in the first and second scheduling levels, the
+ * first level's iteration budget, threads per fit of the FP64 re-runs --
+ * by coordinate descent with CUDA events (median of three calls per shape),
+ * and keeps a shape only if it is at least 1 % faster and its rows match the
+ * default shape's (at most one candidate in 10^4 with another reject code or
+ * a position moved by 1e-3 px or more: the launch shape changes the FP32
+ * summation order, nothing else). The winner is stored in the context for
+ * `method` and used by later fit calls of that method wherever their
+ * options leave these fields at 0. `base` supplies every other option
+ * (NULL: defaults). Blocks until done; allocates its own output buffers.
+ */
+typedef struct loc_tuning {
+    int32_t threads_per_fit;
+    int32_t tail_threads_per_fit;
+    int32_t level0_budget;
+    int32_t rerun_threads_per_fit;
+    int32_t long_rerun_threads_per_fit;
+    int32_t threads_per_block;
+    float ms_default;          /* device time of one call on the sample, default shape */
+    float ms_tuned;            /* ... tuned shape */
+    int32_t trials;            /* shapes timed */
+    int32_t flag_changes;      /* reject codes that differ from the default shape's */
+    int32_t position_changes;  /* kept positions that moved by >= 1e-3 px */
+} loc_tuning;
+LOC_API int loc_autotune(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, int n_rows, int n_cols,
+                         const loc_candidate *d_cands, int n_cands, int method, double w0, double sigma,
+                         const loc_options *base, loc_tuning *result, void *stream);
 
 /* Wait for all work of the context on `stream` and report device errors. */
 LOC_API int loc_sync(loc_ctx *ctx, void *stream);

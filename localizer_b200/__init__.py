@@ -53,7 +53,8 @@ class Options(C.Structure):
                 ("threads_per_fit", C.c_int32), ("tail_threads_per_fit", C.c_int32), ("level0_budget", C.c_int32),
                 ("fp64_rerun", C.c_int32), ("rerun_margin", C.c_float), ("rerun_pivot", C.c_float),
                 ("rerun_threads_per_fit", C.c_int32), ("serial_classes", C.c_int32),
-                ("proposal", C.c_void_p), ("warm_iter_limit", C.c_int32)]
+                ("proposal", C.c_void_p), ("warm_iter_limit", C.c_int32), ("long_rerun_iters", C.c_int32),
+                ("long_rerun_threads_per_fit", C.c_int32), ("compensated", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -68,6 +69,17 @@ class Stats(C.Structure):
     def as_dict(self):
         return {n: (float(getattr(self, n)) if n.endswith("_ms") else int(getattr(self, n)))
                 for n, _ in self._fields_}
+
+
+class Tuning(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("threads_per_fit", "tail_threads_per_fit", "level0_budget",
+                                         "rerun_threads_per_fit", "long_rerun_threads_per_fit",
+                                         "threads_per_block")] + \
+               [("ms_default", C.c_float), ("ms_tuned", C.c_float)] + \
+               [(n, C.c_int32) for n in ("trials", "flag_changes", "position_changes")]
+
+    def as_dict(self):
+        return {n: (float(getattr(self, n)) if n.startswith("ms_") else int(getattr(self, n))) for n, _ in self._fields_}
 
 
 # names and prototypes of every exported entry point of include/localizer_b200.h
@@ -90,6 +102,8 @@ _PROTOS = {
                                        C.c_double, C.c_double, C.POINTER(Options), C.c_void_p, C.c_void_p,
                                        C.c_void_p]),
     "loc_sync": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "loc_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                               C.c_double, C.c_double, C.POINTER(Options), C.POINTER(Tuning), C.c_void_p]),
     "loc_last_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "loc_compact_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int]),
     "loc_find_candidates_host": (C.c_long, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
@@ -205,6 +219,16 @@ class Engine:
         _check(lib().loc_fit_batch(self._h, C.c_void_p(d_frames), n_frames, n_rows, n_cols, C.c_void_p(d_cands),
                                    n_cands, method, w0, sigma, C.byref(o), C.c_void_p(d_out), C.c_void_p(d_flags),
                                    C.c_void_p(stream)))
+
+    def autotune(self, d_frames: int, n_frames: int, n_rows: int, n_cols: int, d_cands: int, n_cands: int,
+                 method: int, w0: float, sigma: float = 1.0, options: Options | None = None, stream: int = 0) -> dict:
+        """loc_autotune on a device sample; the tuned shape is kept in this
+        context for `method`. Returns the loc_tuning fields."""
+        t = Tuning()
+        _check(lib().loc_autotune(self._h, C.c_void_p(d_frames), n_frames, n_rows, n_cols, C.c_void_p(d_cands),
+                                  n_cands, method, w0, sigma, C.byref(options) if options is not None else None,
+                                  C.byref(t), C.c_void_p(stream)))
+        return t.as_dict()
 
     def sync(self, stream: int = 0):
         _check(lib().loc_sync(self._h, C.c_void_p(stream)))

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -73,6 +74,15 @@ struct loc_ctx {
     cudaStream_t aux[locb::kMaxAux] = {};
     cudaEvent_t fork = nullptr;
     cudaEvent_t join[locb::kMaxAux] = {};
+    cudaStream_t aux_long[locb::kMaxAux] = {};
+    cudaEvent_t flagged[locb::kMaxAux] = {};
+    cudaEvent_t join_long[locb::kMaxAux] = {};
+    // launch shapes picked by loc_autotune, per method code; applied where
+    // a call leaves the corresponding option at 0
+    struct Shape {
+        bool set = false;
+        int tpf = 1, tail_tpf = 8, budget = 32, rerun_tpf = 2, long_tpf = 8, tpb = 128;
+    } tuned[8];
     // loc_fit_host_async: two device slots used in turn, and one stream each
     // for uploads, fits and downloads, so that a call's upload runs while the
     // previous call fits and its download while the next call fits
@@ -144,7 +154,10 @@ LOC_API int loc_ctx_create(loc_ctx **ctx, int device)
         return cuda_fail(e, "cudaEventCreate");
     for (int k = 0; k < locb::kMaxAux; ++k) {
         if ((e = cudaStreamCreateWithFlags(&c->aux[k], cudaStreamNonBlocking)) != cudaSuccess ||
-            (e = cudaEventCreateWithFlags(&c->join[k], cudaEventDisableTiming)) != cudaSuccess)
+            (e = cudaEventCreateWithFlags(&c->join[k], cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&c->aux_long[k], cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&c->flagged[k], cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&c->join_long[k], cudaEventDisableTiming)) != cudaSuccess)
             return cuda_fail(e, "auxiliary stream");
     }
     *ctx = c;
@@ -167,6 +180,9 @@ LOC_API int loc_ctx_destroy(loc_ctx *ctx)
     for (int k = 0; k < locb::kMaxAux; ++k) {
         if (ctx->aux[k]) cudaStreamDestroy(ctx->aux[k]);
         if (ctx->join[k]) cudaEventDestroy(ctx->join[k]);
+        if (ctx->aux_long[k]) cudaStreamDestroy(ctx->aux_long[k]);
+        if (ctx->flagged[k]) cudaEventDestroy(ctx->flagged[k]);
+        if (ctx->join_long[k]) cudaEventDestroy(ctx->join_long[k]);
     }
     for (cudaStream_t s : {ctx->s_in, ctx->s_fit, ctx->s_out})
         if (s) {
@@ -211,6 +227,15 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     else loc_default_options(&o);
     if (o.max_iter < 1) return fail(LOC_E_INVALID, "max_iter < 1");
     if (!(o.epsrel >= 0) || !(o.epsabs >= 0)) return fail(LOC_E_INVALID, "negative tolerance");
+    const loc_ctx::Shape &tu = ctx->tuned[method];
+    if (tu.set) {
+        if (o.threads_per_fit == 0) o.threads_per_fit = tu.tpf;
+        if (o.tail_threads_per_fit == 0) o.tail_threads_per_fit = tu.tail_tpf;
+        if (o.level0_budget == 0) o.level0_budget = tu.budget;
+        if (o.rerun_threads_per_fit == 0) o.rerun_threads_per_fit = tu.rerun_tpf;
+        if (o.long_rerun_threads_per_fit == 0) o.long_rerun_threads_per_fit = tu.long_tpf;
+        if (o.threads_per_block == 0) o.threads_per_block = tu.tpb;
+    }
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
     const int rerun = o.fp64_rerun >= 0 ? 1 : 0;
@@ -246,14 +271,22 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     p.threads_per_block = o.threads_per_block;
     p.blocks_per_sm = o.blocks_per_sm;
     p.max_half_width = o.max_half_width;
-    p.threads_per_fit = o.threads_per_fit > 0 ? o.threads_per_fit : 1;
+    p.threads_per_fit = o.threads_per_fit > 0 ? o.threads_per_fit : (o.compensated > 0 ? 4 : 1);
+    if (o.compensated > 0 && p.threads_per_fit < 4) p.threads_per_fit = 4;
     p.tail_threads_per_fit = o.tail_threads_per_fit > 0 ? o.tail_threads_per_fit : 8;
     p.level0_budget = o.level0_budget == 0 ? 32 : (o.level0_budget < 0 ? 0 : o.level0_budget);
     p.fp64_rerun = rerun;
     p.rerun_threads_per_fit = (o.rerun_threads_per_fit == 1 || o.rerun_threads_per_fit == 4 ||
                                o.rerun_threads_per_fit == 8) ? o.rerun_threads_per_fit : 2;
+    p.compensated = o.compensated > 0 ? 1 : 0;
     p.rerun_margin = o.rerun_margin > 0 ? o.rerun_margin : 1e-4f;
     p.rerun_pivot = o.rerun_pivot > 0 ? o.rerun_pivot : 1e-4f;
+    p.long_rerun_threads_per_fit = o.long_rerun_threads_per_fit > 0 ? o.long_rerun_threads_per_fit : 8;
+    p.long_rerun_iters = o.long_rerun_iters == 0 ? (p.level0_budget > 0 ? p.level0_budget : 32)
+                                                 : (o.long_rerun_iters < 0 ? 0 : o.long_rerun_iters);
+    if (!(p.long_rerun_threads_per_fit == 1 || p.long_rerun_threads_per_fit == 2 ||
+          p.long_rerun_threads_per_fit == 4 || p.long_rerun_threads_per_fit == 8))
+        return fail(LOC_E_INVALID, "long_rerun_threads_per_fit must be 1, 2, 4 or 8");
     if (!(p.threads_per_fit == 1 || p.threads_per_fit == 4 || p.threads_per_fit == 8) ||
         !(p.tail_threads_per_fit == 1 || p.tail_threads_per_fit == 4 || p.tail_threads_per_fit == 8))
         return fail(LOC_E_INVALID, "threads per fit must be 1, 4 or 8");
@@ -274,6 +307,9 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     for (int k = 0; k < locb::kMaxAux; ++k) {
         p.aux[k] = o.serial_classes ? nullptr : ctx->aux[k];
         p.join[k] = ctx->join[k];
+        p.aux_long[k] = o.serial_classes ? nullptr : ctx->aux_long[k];
+        p.flagged[k] = ctx->flagged[k];
+        p.join_long[k] = ctx->join_long[k];
     }
     p.fork = ctx->fork;
     p.out = d_out;
@@ -284,6 +320,160 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     if (e != cudaSuccess) {
         if (detail == 1) return fail(LOC_E_UNSUPPORTED, "ROI too large for shared memory");
         return cuda_fail(e, "fit launch");
+    }
+    return LOC_OK;
+}
+
+namespace {
+
+// Device buffer owned by one loc_autotune call.
+struct TuneBuf {
+    void *p = nullptr;
+    ~TuneBuf() { if (p) cudaFree(p); }
+};
+
+// Rows of a trial shape against the default shape's: reject codes and
+// positions (x, y columns) of the fits both keep. A shape is admissible when
+// at most one fit in 10^4 (at least one) changes its reject code and at most
+// as many kept positions move by 1e-3 px or more.
+bool same_results(const std::vector<double> &a, const std::vector<uint8_t> &fa, const std::vector<double> &b,
+                  const std::vector<uint8_t> &fb, int ncol, int xcol, long *n_flag, long *n_pos)
+{
+    const size_t n = fa.size();
+    long df = 0, dp = 0;
+    for (size_t i = 0; i < n; ++i) {
+        if ((fa[i] == 0) != (fb[i] == 0)) {
+            ++df;
+            continue;
+        }
+        if (fa[i] != 0) continue;
+        const double dx = std::fabs(a[i * ncol + xcol] - b[i * ncol + xcol]);
+        const double dy = std::fabs(a[i * ncol + xcol + 1] - b[i * ncol + xcol + 1]);
+        if (!(dx < 1e-3 && dy < 1e-3)) ++dp;
+    }
+    *n_flag = df;
+    *n_pos = dp;
+    const long lim = std::max<long>(1, (long)(n / 10000));
+    return df <= lim && dp <= lim;
+}
+
+}  // namespace
+
+LOC_API int loc_autotune(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, int n_rows, int n_cols,
+                         const loc_candidate *d_cands, int n_cands, int method, double w0, double sigma,
+                         const loc_options *base, loc_tuning *result, void *stream)
+{
+    int dummy = 0;
+    int rc = validate(ctx, d_frames, n_frames, n_rows, n_cols, d_cands, n_cands, method, w0, sigma, &dummy, &dummy);
+    if (rc) return rc;
+    if (method == LOC_METHOD_MLEWG) return fail(LOC_E_UNSUPPORTED, "MLEwG has no launch shape to tune");
+    if (n_cands < 1) return fail(LOC_E_INVALID, "the tuning sample is empty");
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    const cudaStream_t st = (cudaStream_t)stream;
+    loc_options b;
+    if (base) b = *base;
+    else loc_default_options(&b);
+    if (b.precision == LOC_PRECISION_FP64) return fail(LOC_E_UNSUPPORTED, "the tuner times the FP32 solver");
+    const int ncol = loc_output_columns(method);
+    const int xcol = method == 0 ? 3 : method == 1 ? 2 : 4;
+    TuneBuf out, flg;
+    if ((e = cudaMalloc(&out.p, sizeof(double) * (size_t)n_cands * ncol)) != cudaSuccess ||
+        (e = cudaMalloc(&flg.p, (size_t)n_cands)) != cudaSuccess)
+        return fail(LOC_E_NOMEM, std::string("tuning buffers: ") + cudaGetErrorString(e));
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    if ((e = cudaEventCreate(&t0)) != cudaSuccess || (e = cudaEventCreate(&t1)) != cudaSuccess) {
+        if (t0) cudaEventDestroy(t0);
+        return cuda_fail(e, "tuning events");
+    }
+    ctx->tuned[method].set = false;   // zeros mean the built-in defaults while tuning
+    std::vector<double> rows_ref((size_t)n_cands * ncol), rows((size_t)n_cands * ncol);
+    std::vector<uint8_t> flags_ref(n_cands), flags(n_cands);
+    int trials = 0;
+    // median device time of three calls after one untimed call; rows and
+    // flags of the last call copied to the host
+    auto time_shape = [&](const loc_ctx::Shape &sh, float *ms, std::vector<double> &r,
+                          std::vector<uint8_t> &f) -> int {
+        loc_options o = b;
+        o.threads_per_fit = sh.tpf;
+        o.tail_threads_per_fit = sh.tail_tpf;
+        o.level0_budget = sh.budget;
+        o.rerun_threads_per_fit = sh.rerun_tpf;
+        o.long_rerun_threads_per_fit = sh.long_tpf;
+        o.threads_per_block = sh.tpb;
+        float t[3];
+        for (int k = 0; k < 4; ++k) {
+            if (k > 0) cudaEventRecord(t0, st);
+            int r2 = loc_fit_batch(ctx, d_frames, n_frames, n_rows, n_cols, d_cands, n_cands, method, w0, sigma, &o,
+                                   (double *)out.p, (uint8_t *)flg.p, stream);
+            if (r2) return r2;
+            if (k > 0) {
+                cudaEventRecord(t1, st);
+                cudaError_t e2 = cudaEventSynchronize(t1);
+                if (e2 != cudaSuccess) return cuda_fail(e2, "tuning run");
+                cudaEventElapsedTime(&t[k - 1], t0, t1);
+            }
+        }
+        std::sort(t, t + 3);
+        *ms = t[1];
+        ++trials;
+        cudaError_t e2 = cudaMemcpy(r.data(), out.p, sizeof(double) * r.size(), cudaMemcpyDeviceToHost);
+        if (e2 == cudaSuccess) e2 = cudaMemcpy(f.data(), flg.p, f.size(), cudaMemcpyDeviceToHost);
+        if (e2 != cudaSuccess) return cuda_fail(e2, "tuning rows");
+        return LOC_OK;
+    };
+    loc_ctx::Shape best;   // the built-in defaults
+    float best_ms = 0.0f;
+    long worst_flag = 0, worst_pos = 0;
+    rc = time_shape(best, &best_ms, rows_ref, flags_ref);
+    const float ms_default = best_ms;
+    // coordinate descent: each knob in turn over its values, the others held
+    // at the best shape so far; a value must be 1 % faster and give the
+    // default shape's results
+    const std::vector<std::pair<int loc_ctx::Shape::*, std::vector<int>>> knobs = {
+        {&loc_ctx::Shape::tpb, {128, 96, 64}},
+        {&loc_ctx::Shape::tpf, {1, 4, 8}},
+        {&loc_ctx::Shape::budget, {16, 24, 32, 48, 64}},
+        {&loc_ctx::Shape::tail_tpf, {8, 4}},
+        {&loc_ctx::Shape::rerun_tpf, {2, 1, 4}},
+        {&loc_ctx::Shape::long_tpf, {8, 4, 2}},
+    };
+    for (size_t kk = 0; rc == LOC_OK && kk < knobs.size(); ++kk) {
+        const auto &kn = knobs[kk];
+        for (int v : kn.second) {
+            if (rc != LOC_OK || best.*(kn.first) == v) continue;
+            loc_ctx::Shape trial = best;
+            trial.*(kn.first) = v;
+            float ms = 0.0f;
+            rc = time_shape(trial, &ms, rows, flags);
+            if (rc != LOC_OK) break;
+            long nf = 0, np = 0;
+            const bool same = same_results(rows, flags, rows_ref, flags_ref, ncol, xcol, &nf, &np);
+            if (same && ms < 0.99f * best_ms) {
+                best = trial;
+                best_ms = ms;
+                worst_flag = std::max(worst_flag, nf);
+                worst_pos = std::max(worst_pos, np);
+            }
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rc != LOC_OK) return rc;
+    best.set = true;
+    ctx->tuned[method] = best;
+    if (result) {
+        result->threads_per_fit = best.tpf;
+        result->tail_threads_per_fit = best.tail_tpf;
+        result->level0_budget = best.budget;
+        result->rerun_threads_per_fit = best.rerun_tpf;
+        result->long_rerun_threads_per_fit = best.long_tpf;
+        result->threads_per_block = best.tpb;
+        result->ms_default = ms_default;
+        result->ms_tuned = best_ms;
+        result->trials = trials;
+        result->flag_changes = (int32_t)worst_flag;
+        result->position_changes = (int32_t)worst_pos;
     }
     return LOC_OK;
 }

@@ -400,8 +400,12 @@ __device__ __forceinline__ void pass_ell(const float *__restrict__ roi, int ld, 
 // Result codes: 0 ok, 1 an FP32 pivot fell below thr * diagonal (redo in
 // FP64), 2 not positive definite (in the precision T).
 // ---------------------------------------------------------------------------
-template <int P, typename T, typename MS>
-__device__ __forceinline__ int chol_solve(const MS (&Ms)[tri(P)], MS par, const MS (&g)[P], T thr,
+// The triangular loops run over 0..P-1 with the bound as a condition
+// (same operations, same order): with trip counts that depend on the outer
+// index the compiler kept the factor and solve vectors in local memory for
+// P = 7.
+template <int P, typename T, typename MS, typename MA>
+__device__ __forceinline__ int chol_solve(const MA &Ms, MS par, const MS (&g)[P], T thr,
                                           MS (&z)[P], MS &znorm, MS &w2, MS &minpiv)
 {
     T L[tri(P)];
@@ -414,7 +418,8 @@ __device__ __forceinline__ int chol_solve(const MS (&Ms)[tri(P)], MS par, const 
         const T djj = (T)Ms[pku(P, j, j)] + (T)par;
         T d = djj;
 #pragma unroll
-        for (int k = 0; k < j; ++k) d -= L[pkl(j, k)] * L[pkl(j, k)];
+        for (int k = 0; k < P; ++k)
+            if (k < j) d -= L[pkl(j, k)] * L[pkl(j, k)];
         if (d * mpd < mpn * djj) {
             mpn = d;
             mpd = djj;
@@ -427,10 +432,12 @@ __device__ __forceinline__ int chol_solve(const MS (&Ms)[tri(P)], MS par, const 
         inv[j] = il;
         L[pkl(j, j)] = d * il;
 #pragma unroll
-        for (int i = j + 1; i < P; ++i) {
+        for (int i = 0; i < P; ++i) {
+            if (i <= j) continue;
             T sacc = (T)Ms[pku(P, j, i)];
 #pragma unroll
-            for (int k = 0; k < j; ++k) sacc -= L[pkl(i, k)] * L[pkl(j, k)];
+            for (int k = 0; k < P; ++k)
+                if (k < j) sacc -= L[pkl(i, k)] * L[pkl(j, k)];
             L[pkl(i, j)] = sacc * inv[j];
         }
     }
@@ -440,7 +447,8 @@ __device__ __forceinline__ int chol_solve(const MS (&Ms)[tri(P)], MS par, const 
     for (int i = 0; i < P; ++i) {
         T sacc = (T)g[i];
 #pragma unroll
-        for (int k = 0; k < i; ++k) sacc -= L[pkl(i, k)] * y[k];
+        for (int k = 0; k < P; ++k)
+            if (k < i) sacc -= L[pkl(i, k)] * y[k];
         y[i] = sacc * inv[i];
     }
     T zz[P];
@@ -448,7 +456,8 @@ __device__ __forceinline__ int chol_solve(const MS (&Ms)[tri(P)], MS par, const 
     for (int ii = P - 1; ii >= 0; --ii) {
         T sacc = y[ii];
 #pragma unroll
-        for (int k = ii + 1; k < P; ++k) sacc -= L[pkl(k, ii)] * zz[k];
+        for (int k = 0; k < P; ++k)
+            if (k > ii) sacc -= L[pkl(k, ii)] * zz[k];
         zz[ii] = sacc * inv[ii];
     }
     T n2 = T(0);
@@ -463,7 +472,8 @@ __device__ __forceinline__ int chol_solve(const MS (&Ms)[tri(P)], MS par, const 
         for (int i = 0; i < P; ++i) {
             T sacc = zz[i] * izn;
 #pragma unroll
-            for (int k = 0; k < i; ++k) sacc -= L[pkl(i, k)] * qv[k];
+            for (int k = 0; k < P; ++k)
+                if (k < i) sacc -= L[pkl(i, k)] * qv[k];
             qv[i] = sacc * inv[i];
             q2 += qv[i] * qv[i];
         }
@@ -495,15 +505,18 @@ __device__ __noinline__ int chol_solve_fp64(const float *Ms, float par, const fl
     return rc;
 }
 
-// One damped solve in working precision T with FP64 escalation for float.
-template <int P, typename T>
-__device__ __forceinline__ int damped_solve(const T (&Ms)[tri(P)], T par, const T (&g)[P], float thr,
+// One damped solve in working precision T; with ESC (FP32 only), pivots
+// below thr * diagonal are refactorised in FP64. ESC is a separate kernel
+// instantiation: the out-of-line FP64 call costs the solver loop a stack
+// frame and register spills even when it never runs.
+template <int P, typename T, bool ESC, typename MA>
+__device__ __forceinline__ int damped_solve(const MA &Ms, T par, const T (&g)[P], float thr,
                                             T (&z)[P], T &znorm, T &w2, T &minpiv, unsigned &n_esc)
 {
     // FP64 solves take no pivot threshold (there is no higher precision to
     // escalate to), so only FP32 solves can return 1
-    int rc = chol_solve<P, T, T>(Ms, par, g, sizeof(T) == 4 ? (T)thr : T(0), z, znorm, w2, minpiv);
-    if constexpr (sizeof(T) == 4) {
+    int rc = chol_solve<P, T, T>(Ms, par, g, (ESC && sizeof(T) == 4) ? (T)thr : T(0), z, znorm, w2, minpiv);
+    if constexpr (ESC && sizeof(T) == 4) {
         if (rc == 1) {
             ++n_esc;
             float msl[tri(P)], gl[P], zl[P], o2[2];
@@ -532,8 +545,8 @@ __device__ __forceinline__ int damped_solve(const T (&Ms)[tri(P)], T par, const 
 // quantity and the threshold of a branch it decided (the Newton acceptance
 // fp <= 0.1 delta, the |fp| <= 0.1 delta stop, the fp <= fp_old stop): a
 // small margin means a rounding difference could have taken the other branch.
-template <int P, typename T>
-__device__ __forceinline__ void lmpar_scaled(const T (&Ms)[tri(P)], const T (&g)[P], T delta, T &par,
+template <int P, typename T, bool ESC, typename MA>
+__device__ __forceinline__ void lmpar_scaled(const MA &Ms, const T (&g)[P], T delta, T &par,
                                              T (&z)[P], float thr, unsigned &n_lambda, unsigned &n_esc,
                                              bool &singular, T &newton_piv, T &margin)
 {
@@ -553,7 +566,7 @@ __device__ __forceinline__ void lmpar_scaled(const T (&Ms)[tri(P)], const T (&g)
             pr = t > tiny_pos<T>() ? t : tiny_pos<T>();
         }
         ++n_lambda;
-        const int rc = damped_solve<P, T>(Ms, pr, g, thr, z, dxnorm, w2, mp, n_esc);
+        const int rc = damped_solve<P, T, ESC>(Ms, pr, g, thr, z, dxnorm, w2, mp, n_esc);
         if (first) {
             first = false;
             newton_piv = mp;

@@ -166,15 +166,21 @@ __global__ void k3_flag(const float *state32, int stride, const int *cls, const 
 }
 
 // Per-class form of the flag pass: walks the queue of half-width r and
-// appends the flagged fits to that class's FP64 queue (order2 / meta2).
+// appends the flagged fits to that class's FP64 queue (order2 / meta2), or,
+// when their FP32 solve took more than long_iters iterations and a long
+// queue exists (order3 / meta3), to that one: the long fits set the length
+// of the re-run, so they get their own launch with more threads per fit.
 template <int P>
 __global__ void k3_flag_class(const float *state32, int stride, const int *order, const int *meta,
                               const uint8_t *flags, int r, float margin, float pivot, int warm_limit, int *cls2,
-                              int *order2, int *meta2)
+                              int *order2, int *meta2, int long_iters, int *order3, int *meta3)
 {
     using SL = StateLayout<P>;
     const int start = meta[m_start(r)], count = meta[m_count(r)];
-    if (blockIdx.x == 0 && threadIdx.x == 0) meta2[m_start(r)] = start;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        meta2[m_start(r)] = start;
+        if (meta3) meta3[m_start(r)] = start;
+    }
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
         const int i = order[start + t];
         if (flags[i] != F_PENDING) continue;
@@ -187,8 +193,13 @@ __global__ void k3_flag_class(const float *state32, int stride, const int *order
                             (warm_limit > 0 && s[SL::ITERS] > (float)warm_limit));
         if (risky) {
             cls2[i] = r;
-            const int slot = atomicAdd(&meta2[m_count(r)], 1);
-            order2[start + slot] = i;
+            if (meta3 && s[SL::ITERS] > (float)long_iters) {
+                const int slot = atomicAdd(&meta3[m_count(r)], 1);
+                order3[start + slot] = i;
+            } else {
+                const int slot = atomicAdd(&meta2[m_count(r)], 1);
+                order2[start + slot] = i;
+            }
         }
     }
 }
@@ -215,6 +226,7 @@ struct K1Args {
     int *cont;          // continuation queue, laid out like order
     float *cont_state;  // saved solver state of suspended fits
     int cont_stride;
+    int compensated;    // FP32 solver: sum the group's partial normal equations in FP64
 };
 
 template <int METHOD, int S, int TPF, typename T> struct Pass;
@@ -256,6 +268,17 @@ __device__ __forceinline__ T group_sum(T v, int tpf, unsigned mask)
     return v;
 }
 
+// Group sum of FP32 partial sums carried out in FP64 and rounded once: with
+// TPF threads per fit each partial covers 1/TPF of the ROI, so the total is a
+// two-level (pairwise) sum whose rounding error is that of n/TPF terms
+// instead of n.
+__device__ __forceinline__ float group_sum_wide(float v, int tpf, unsigned mask)
+{
+    double d = (double)v;
+    for (int o = tpf >> 1; o > 0; o >>= 1) d += __shfl_xor_sync(mask, d, o);
+    return (float)d;
+}
+
 template <typename T>
 __device__ __forceinline__ T group_max(T v, int tpf, unsigned mask)
 {
@@ -279,22 +302,24 @@ template <typename T, int N> struct StateArr<T, N, false> {
     T r[N];
     __device__ __forceinline__ explicit StateArr(T *) {}
     __device__ __forceinline__ T &operator[](int k) { return r[k]; }
+    __device__ __forceinline__ const T &operator[](int k) const { return r[k]; }
 };
 template <typename T, int N> struct StateArr<T, N, true> {
     T *p;
     __device__ __forceinline__ explicit StateArr(T *slot) : p(slot) {}
     __device__ __forceinline__ T &operator[](int k) { return p[k]; }
+    __device__ __forceinline__ const T &operator[](int k) const { return p[k]; }
 };
 
 // Shared memory of the solver block: the ROIs, then (FP64 only) the
 // per-fit normal equations.
 template <typename T>
-__host__ __device__ constexpr int state_smem_per_fit(int P) { return sizeof(T) == 8 ? (tri(P) + P) * 8 : 0; }
+__host__ __device__ constexpr int state_smem_per_fit(int P) { return sizeof(T) == 8 ? (2 * tri(P) + 4 * P) * 8 : 0; }
 
 // Process one queue of ROI half-width r: the fresh candidates (level 0) or
 // the fits suspended there (level 1). TPF threads cooperate on each fit;
 // S = 2r + 1 at compile time, or 0 for a runtime side.
-template <int METHOD, typename T, int S, int TPF>
+template <int METHOD, typename T, int S, int TPF, bool ESC>
 __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, unsigned (&st)[ST_N])
 {
     constexpr int P = Traits<METHOD>::P;
@@ -326,9 +351,16 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
         const int roi_bytes = (blockDim.x / TPF) * stride * (int)sizeof(float);
         sstate = (T *)((char *)smem + ((roi_bytes + 15) / 16) * 16) + (tid / TPF) * (NT + P);
     }
+    // FP64: the normal equations, parameters, scaling, last step and the
+    // scaled matrix of the damped solve live in the fit's shared-memory slot
+    // (in registers they push the FP64 solver into spills); te, the
+    // evaluation point, stays in registers
     StateArr<T, NT, kSmemState> A(sstate);
-    StateArr<T, P, kSmemState> v(sstate + NT);
-    T th[P], D[P], dx[P], te[P];
+    StateArr<T, P, kSmemState> v(sstate ? sstate + NT : nullptr);
+    StateArr<T, P, kSmemState> th(sstate ? sstate + NT + P : nullptr);
+    StateArr<T, P, kSmemState> D(sstate ? sstate + NT + 2 * P : nullptr);
+    StateArr<T, P, kSmemState> dx(sstate ? sstate + NT + 3 * P : nullptr);
+    T te[P];
     T fnorm = 0, delta = 0, par = 0, xnorm = 0, jdx2 = 0, pnorm = 0;
     int phase = 0, it_state = 0, iterations = 0, trial = 0, cidx = -1, xo = 0, yo = 0;
     T minpiv_fit = T(1);
@@ -340,7 +372,7 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
 #pragma unroll
     for (int k = 0; k < NT; ++k) A[k] = T(0);
 
-    auto theta_abs = [&](int k, const T (&t)[P]) -> T {
+    auto theta_abs = [&](int k, auto &t) -> T {
         return k == IX ? t[k] + (T)xo : (k == IX + 1 ? t[k] + (T)yo : t[k]);
     };
     auto write_finish = [&](int status) {
@@ -557,7 +589,8 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
             do_pass = true;
         } else if (phase == 2) {
             ++trial;
-            T invD[P], g[P], Ms[NT], z[P];
+            T invD[P], g[P], z[P];
+            StateArr<T, NT, kSmemState> Ms(sstate ? sstate + NT + 4 * P : nullptr);
 #pragma unroll
             for (int k = 0; k < P; ++k) {
                 invD[k] = frcp(D[k]);
@@ -570,7 +603,7 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
             unsigned nl = 0, ne = 0;
             bool sing = false;
             T npiv;
-            lmpar_scaled<P, T>(Ms, g, delta, par, z, a.pivot_thr, nl, ne, sing, npiv, margin_fit);
+            lmpar_scaled<P, T, ESC>(Ms, g, delta, par, z, a.pivot_thr, nl, ne, sing, npiv, margin_fit);
             if (leader) {
                 st[ST_LAMBDA] += nl;
                 st[ST_ESC] += ne;
@@ -616,7 +649,23 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
 #pragma unroll
             for (int k = 0; k < P; ++k) dt[k] = phase == 2 ? dx[k] : T(0);
             Pass<METHOD, S, TPF, T>::run(myroi, s, q, w0, te, dt, acc, vv, chi2, dchi, dqmax);
-            if constexpr (TPF > 1) {
+            if constexpr (TPF > 1 && sizeof(T) == 4) {
+                if (a.compensated) {
+#pragma unroll
+                    for (int k = 0; k < NT - 1; ++k) acc[k] = group_sum_wide(acc[k], TPF, pmask);
+#pragma unroll
+                    for (int k = 0; k < P; ++k) vv[k] = group_sum_wide(vv[k], TPF, pmask);
+                    chi2 = group_sum_wide(chi2, TPF, pmask);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < NT - 1; ++k) acc[k] = group_sum(acc[k], TPF, pmask);
+#pragma unroll
+                    for (int k = 0; k < P; ++k) vv[k] = group_sum(vv[k], TPF, pmask);
+                    chi2 = group_sum(chi2, TPF, pmask);
+                }
+                dchi = group_sum(dchi, TPF, pmask);
+                dqmax = group_max(dqmax, TPF, pmask);
+            } else if constexpr (TPF > 1) {
 #pragma unroll
                 for (int k = 0; k < NT - 1; ++k) acc[k] = group_sum(acc[k], TPF, pmask);
 #pragma unroll
@@ -758,14 +807,14 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
 // (FP64: one, i.e. the full 255 registers)
 __host__ __device__ constexpr int k1_min_blocks(int method, int bytes) { return bytes == 8 ? 1 : (method == 7 ? 2 : 3); }
 
-template <int METHOD, typename T, int S, int TPF>
+template <int METHOD, typename T, int S, int TPF, bool ESC>
 __global__ void __launch_bounds__(128, k1_min_blocks(METHOD, sizeof(T))) k1_lm_fit(K1Args a, int r)
 {
     extern __shared__ float smem[];
     unsigned st[ST_N];
 #pragma unroll
     for (int k = 0; k < ST_N; ++k) st[k] = 0;
-    if (a.meta[a.level == 1 ? m_ccount(r) : m_count(r)] > 0) run_class<METHOD, T, S, TPF>(a, r, smem, st);
+    if (a.meta[a.level == 1 ? m_ccount(r) : m_count(r)] > 0) run_class<METHOD, T, S, TPF, ESC>(a, r, smem, st);
     // warp-reduce the counters, one atomic per warp and counter
 #pragma unroll
     for (int k = 0; k < ST_N; ++k) {
@@ -1026,10 +1075,10 @@ __global__ void k2_finalize(K2Args a)
 
 int solver_method(int method) { return method == 5 ? 7 : method; }
 
-template <int METHOD, typename T, int S, int TPF>
+template <int METHOD, typename T, int S, int TPF, bool ESC = false>
 cudaError_t launch_k1_s(const K1Args &ka, int r, int tpb, int bps_req, cudaStream_t stream)
 {
-    auto kern = k1_lm_fit<METHOD, T, S, TPF>;
+    auto kern = k1_lm_fit<METHOD, T, S, TPF, ESC>;
     const int side = 2 * r + 1;
     const int per_fit = roi_stride(side * side, TPF) * (int)sizeof(float);
     constexpr int P = Traits<METHOD>::P;
@@ -1057,6 +1106,9 @@ cudaError_t launch_k1_tpf(const K1Args &ka, int r, int tpb, int bps_req, cudaStr
     if constexpr (sizeof(T) == 8) {
         return launch_k1_s<METHOD, T, 0, TPF>(ka, r, tpb, bps_req, stream);
     } else {
+        // FP64 pivot escalation: one runtime-side instantiation per method
+        // and threads per fit
+        if (ka.pivot_thr > 0.0f) return launch_k1_s<METHOD, T, 0, TPF, true>(ka, r, tpb, bps_req, stream);
         switch (2 * r + 1) {
         case 5: return launch_k1_s<METHOD, T, 5, TPF>(ka, r, tpb, bps_req, stream);
         case 7: return launch_k1_s<METHOD, T, 7, TPF>(ka, r, tpb, bps_req, stream);
@@ -1116,7 +1168,7 @@ size_t scratch_bytes(int method, int n, int precision, int rerun, int warm)
                al256(sizeof(unsigned long long) * kStatWords) + al256(sizeof(int) * (size_t)n) +
                al256(sizeof(float) * (size_t)n * cont_stride_of(m)) + al256(el * (size_t)n * state_stride(method));
     if (precision != 1 && rerun)
-        b += al256(sizeof(int) * (size_t)n) * 2 + al256(sizeof(int) * kMetaInts) +
+        b += al256(sizeof(int) * (size_t)n) * 3 + al256(sizeof(int) * kMetaInts) * 2 +
              al256(sizeof(double) * (size_t)n * state_stride(method));
     if (warm) b += al256(sizeof(float) * (size_t)n * 8);
     return b;
@@ -1147,10 +1199,14 @@ void carve_scratch(void *base, int method, int n, int precision, int rerun, Scra
         p += al256(sizeof(int) * (size_t)n);
         s->meta2 = (int *)p;
         p += al256(sizeof(int) * kMetaInts);
+        s->order3 = (int *)p;
+        p += al256(sizeof(int) * (size_t)n);
+        s->meta3 = (int *)p;
+        p += al256(sizeof(int) * kMetaInts);
         s->state64 = (double *)p;
         p += al256(sizeof(double) * (size_t)n * state_stride(method));
     } else {
-        s->cls2 = s->order2 = s->meta2 = nullptr;
+        s->cls2 = s->order2 = s->meta2 = s->order3 = s->meta3 = nullptr;
         s->state64 = nullptr;
     }
     s->init = warm ? (float *)p : nullptr;
@@ -1195,6 +1251,8 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
     e = cudaMemsetAsync(s.meta, 0, sizeof(int) * kMetaInts, stream);
     if (e != cudaSuccess) return e;
     if (rerun && (e = cudaMemsetAsync(s.meta2, 0, sizeof(int) * kMetaInts, stream)) != cudaSuccess) return e;
+    const bool long_q = rerun && p.long_rerun_iters > 0;
+    if (long_q && (e = cudaMemsetAsync(s.meta3, 0, sizeof(int) * kMetaInts, stream)) != cudaSuccess) return e;
     e = cudaMemsetAsync(s.stats, 0, sizeof(unsigned long long) * kStatWords, stream);
     if (e != cudaSuccess) return e;
     if (p.method == 6) {
@@ -1255,7 +1313,7 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
               s.state, state_stride(p.method), (float)p.w0, (float)(1.0 / (p.sigma * p.sigma)),
               (float)(1.0 / s_abs), 1.0 / (p.sigma * p.sigma), 1.0 / s_abs, p.max_iter, (float)p.epsabs,
               (float)p.epsrel, p.precision == 1 ? 0.0f : p.pivot_thr, p.warm ? s.init : p.init_params, s.stats,
-              0, 0, s.cont, s.cont_state, cont_stride_of(m)};
+              0, 0, s.cont, s.cont_state, cont_stride_of(m), p.compensated};
     // Each ROI class is an independent chain -- level 0 (every candidate,
     // tpf0 threads per fit, up to `budget` iterations), level 1 (the fits
     // still running, tpf1 threads per fit), the flag pass and the FP64
@@ -1269,13 +1327,13 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
         e = cudaEventRecord(p.fork, stream);
         if (e != cudaSuccess) return e;
     }
-    bool used[kMaxAux] = {false};
+    bool used[kMaxAux] = {false}, used_long[kMaxAux] = {false};
     int chain = 0;
     for (int r = r_cap; r >= 1; --r) {
         if (counts[r] <= 0) continue;
         cudaStream_t cs = stream;
+        const int j = naux > 0 ? chain % naux : 0;
         if (naux > 0) {
-            const int j = chain % naux;
             cs = p.aux[j];
             if (!used[j]) {
                 if ((e = cudaStreamWaitEvent(cs, p.fork, 0)) != cudaSuccess) return e;
@@ -1294,14 +1352,18 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
                 const int wl = p.warm ? p.warm_iter_limit : 0;
                 const float *st32 = (const float *)s.state;
                 const int sst = state_stride(p.method);
+                int *o3 = long_q ? s.order3 : nullptr, *m3 = long_q ? s.meta3 : nullptr;
+                const int li = p.long_rerun_iters;
                 switch (m) {
                 case 0: k3_flag_class<5><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r, p.rerun_margin,
-                                                             p.rerun_pivot, wl, s.cls2, s.order2, s.meta2); break;
+                                                             p.rerun_pivot, wl, s.cls2, s.order2, s.meta2, li, o3,
+                                                             m3); break;
                 case 1: k3_flag_class<4><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r, p.rerun_margin,
-                                                             p.rerun_pivot, wl, s.cls2, s.order2, s.meta2); break;
+                                                             p.rerun_pivot, wl, s.cls2, s.order2, s.meta2, li, o3,
+                                                             m3); break;
                 default: k3_flag_class<7><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r,
                                                               p.rerun_margin, p.rerun_pivot, wl, s.cls2, s.order2,
-                                                              s.meta2); break;
+                                                              s.meta2, li, o3, m3); break;
                 }
                 if ((e = cudaGetLastError()) != cudaSuccess) return e;
                 bump();
@@ -1313,16 +1375,39 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
                 k64.state = s.state64;
                 k64.pivot_thr = 0.0f;
                 k64.stats = s.stats + ST_N;  // counters of the re-run kept apart
-                // the flagged fits are the long, hard ones: several threads per fit
+                if (long_q) {
+                    // the long re-runs: their own stream (when the chain has
+                    // one) and more threads per fit; launched first so that
+                    // in a serial call they start at the head
+                    K1Args kl = k64;
+                    kl.order = s.order3;
+                    kl.meta = s.meta3;
+                    cudaStream_t ls = cs;
+                    if (naux > 0 && p.aux_long[j]) {
+                        ls = p.aux_long[j];
+                        if ((e = cudaEventRecord(p.flagged[j], cs)) != cudaSuccess) return e;
+                        if ((e = cudaStreamWaitEvent(ls, p.flagged[j], 0)) != cudaSuccess) return e;
+                        used_long[j] = true;
+                    }
+                    e = launch_queues<double>(p, kl, cnt1, r_cap, tpb, false, p.long_rerun_threads_per_fit, ls,
+                                              err_detail);
+                    if (e != cudaSuccess) return e;
+                }
+                // the other flagged fits: fewer threads per fit, more fits in flight
                 e = launch_queues<double>(p, k64, cnt1, r_cap, tpb, false, p.rerun_threads_per_fit, cs, err_detail);
             }
         }
         if (e != cudaSuccess) return e;
     }
     for (int j = 0; j < naux; ++j) {
-        if (!used[j]) continue;
-        if ((e = cudaEventRecord(p.join[j], p.aux[j])) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(stream, p.join[j], 0)) != cudaSuccess) return e;
+        if (used[j]) {
+            if ((e = cudaEventRecord(p.join[j], p.aux[j])) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(stream, p.join[j], 0)) != cudaSuccess) return e;
+        }
+        if (used_long[j]) {
+            if ((e = cudaEventRecord(p.join_long[j], p.aux_long[j])) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(stream, p.join_long[j], 0)) != cudaSuccess) return e;
+        }
     }
     if (e != cudaSuccess) return e;
     mark(2);

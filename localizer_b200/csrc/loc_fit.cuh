@@ -22,8 +22,10 @@ struct Scratch {
     int *cont;           // n: continuation queue (fits suspended after the level-0 budget)
     float *cont_state;   // n * cont stride: their saved solver state
     int *cls2;           // n: half-width class of fits re-run in FP64, -1 otherwise
-    int *order2;         // n: their queue
+    int *order2;         // n: their queue (fits whose FP32 solve ended within the level-0 budget)
     int *meta2;          // kMetaInts: its class table
+    int *order3;         // n: queue of the long re-runs (FP32 solve outlived the level-0 budget)
+    int *meta3;          // kMetaInts: its class table
     double *state64;     // n * state_stride(method): FP64 state of re-run fits
     float *init;         // n * P: proposed starts (warm mode only)
 };
@@ -49,6 +51,10 @@ struct FitParams {
     int level0_budget;         // iterations before a fit moves to level 1 (0: single level)
     int fp64_rerun;            // re-run flagged FP32 fits in FP64
     int rerun_threads_per_fit; // 1, 2, 4 or 8
+    int long_rerun_threads_per_fit; // 1, 2, 4 or 8: re-runs of fits whose FP32 solve took more
+                                    // than long_rerun_iters iterations
+    int long_rerun_iters;      // 0: no separate long queue
+    int compensated;           // FP32 group sums of the normal equations in FP64 (threads per fit > 1)
     float rerun_margin;        // branch-decision margin below which a fit is flagged
     float rerun_pivot;         // undamped pivot ratio below which a fit is flagged
     const float *init_params;
@@ -63,6 +69,9 @@ struct FitParams {
     cudaStream_t aux[kMaxAux];  // optional auxiliary streams (NULL-terminated) for the class chains
     cudaEvent_t fork;           // fork / join events for them
     cudaEvent_t join[kMaxAux];
+    cudaStream_t aux_long[kMaxAux];  // optional streams for the long FP64 re-runs, one per chain
+    cudaEvent_t flagged[kMaxAux];    // chain j's flag pass done
+    cudaEvent_t join_long[kMaxAux];
     double *out;
     uint8_t *flags;
 };

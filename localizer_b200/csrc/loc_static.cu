@@ -55,6 +55,9 @@ static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBy
 // resolved once per device; the address does not survive cudaDeviceReset
 // (the module is loaded again and the array may move), so a process that
 // resets a device must not call this entry point on it afterwards
+// resolved once per device; the address does not survive cudaDeviceReset
+// (the module is loaded again and the array may move), so a process that
+// resets a device must not call this entry point on it afterwards
 void *g_scratch_ptr[kMaxDevices] = {};
 std::mutex g_setup_mu;
 
@@ -88,7 +91,8 @@ extern "C" LOC_API int loc_fit_batch_static(const uint16_t *d_frames, int n_fram
     if (o.max_iter < 1) return err(LOC_E_INVALID, "max_iter < 1");
     if (!(o.epsrel >= 0) || !(o.epsabs >= 0)) return err(LOC_E_INVALID, "negative tolerance");
     if (o.proposal) return err(LOC_E_UNSUPPORTED, "start proposals need a context (loc_fit_batch)");
-    const int tpf0 = o.threads_per_fit > 0 ? o.threads_per_fit : 1;
+    int tpf0 = o.threads_per_fit > 0 ? o.threads_per_fit : (o.compensated > 0 ? 4 : 1);
+    if (o.compensated > 0 && tpf0 < 4) tpf0 = 4;
     const int tpf1 = o.tail_threads_per_fit > 0 ? o.tail_threads_per_fit : 8;
     if (!(tpf0 == 1 || tpf0 == 4 || tpf0 == 8) || !(tpf1 == 1 || tpf1 == 4 || tpf1 == 8))
         return err(LOC_E_INVALID, "threads per fit must be 1, 4 or 8");
@@ -141,6 +145,11 @@ extern "C" LOC_API int loc_fit_batch_static(const uint16_t *d_frames, int n_fram
     p.fp64_rerun = rerun;
     p.rerun_threads_per_fit = (o.rerun_threads_per_fit == 1 || o.rerun_threads_per_fit == 4 ||
                                o.rerun_threads_per_fit == 8) ? o.rerun_threads_per_fit : 2;
+    p.long_rerun_threads_per_fit = (o.long_rerun_threads_per_fit == 1 || o.long_rerun_threads_per_fit == 2 ||
+                                    o.long_rerun_threads_per_fit == 4) ? o.long_rerun_threads_per_fit : 8;
+    p.long_rerun_iters = o.long_rerun_iters == 0 ? (p.level0_budget > 0 ? p.level0_budget : 32)
+                                                 : (o.long_rerun_iters < 0 ? 0 : o.long_rerun_iters);
+    p.compensated = o.compensated > 0 ? 1 : 0;
     p.rerun_margin = o.rerun_margin > 0 ? o.rerun_margin : 1e-4f;
     p.rerun_pivot = o.rerun_pivot > 0 ? o.rerun_pivot : 1e-4f;
     p.init_params = o.d_init_params;

@@ -218,12 +218,13 @@ def workload_windows(n_frames: int, method: int, seed: int, pfa: float = 30.0, w
     uneven one by default; seeded, disjoint from the evaluation seeds),
     labelled by the plain LM fit of their candidates at the candidates' own
     ROI half-widths."""
-    from . import find_candidates
+    from . import find_candidates_device
     from . import synth
     w = synth.scaled(synth.workloads()[workload], n_frames, seed=seed)
     frames, _ = synth.make_device(w)
-    host = frames.cpu().numpy().view(np.uint16)
-    cands = find_candidates(host, pfa, w.w0)
+    raw, _ = find_candidates_device(frames, pfa, w.w0)
+    cands = raw.cpu().numpy().view(CANDIDATE_DTYPE).copy()
+    del raw
     cands["half_width"] = np.random.default_rng(seed + 17).choice(np.array(w.half_widths), size=len(cands))
     labels, valid = frame_labels(frames, cands, method, w.w0)
     rois = frame_windows(frames, cands)
