@@ -108,6 +108,23 @@ __device__ __forceinline__ double frsqrt(double a) { return rsqrt(a); }
 __device__ __forceinline__ float fsqrt(float a) { return a > 0.0f ? a * rsqrtf(a) : sqrtf(a); }
 __device__ __forceinline__ double fsqrt(double a) { return sqrt(a); }
 
+// Per-fit array in registers, or (InSmem) in a shared-memory slot of the
+// fit's group; the FP64 solver keeps its normal equations, state vectors and
+// Cholesky factor there so that they are not live in registers.
+template <typename T, int N, bool InSmem> struct StateArr;
+template <typename T, int N> struct StateArr<T, N, false> {
+    T r[N];
+    __device__ __forceinline__ explicit StateArr(T *) {}
+    __device__ __forceinline__ T &operator[](int k) { return r[k]; }
+    __device__ __forceinline__ const T &operator[](int k) const { return r[k]; }
+};
+template <typename T, int N> struct StateArr<T, N, true> {
+    T *p;
+    __device__ __forceinline__ explicit StateArr(T *slot) : p(slot) {}
+    __device__ __forceinline__ T &operator[](int k) { return p[k]; }
+    __device__ __forceinline__ const T &operator[](int k) const { return p[k]; }
+};
+
 template <typename T> __device__ __forceinline__ T tiny_pos();
 template <> __device__ __forceinline__ float tiny_pos<float>() { return FLT_MIN; }
 template <> __device__ __forceinline__ double tiny_pos<double>() { return DBL_MIN; }
@@ -406,9 +423,11 @@ __device__ __forceinline__ void pass_ell(const float *__restrict__ roi, int ld, 
 // P = 7.
 template <int P, typename T, typename MS, typename MA>
 __device__ __forceinline__ int chol_solve(const MA &Ms, MS par, const MS (&g)[P], T thr,
-                                          MS (&z)[P], MS &znorm, MS &w2, MS &minpiv)
+                                          MS (&z)[P], MS &znorm, MS &w2, MS &minpiv, T *lslot = nullptr)
 {
-    T L[tri(P)];
+    // the all-FP64 solve keeps its factor in the fit's shared-memory slot
+    constexpr bool kSm = sizeof(T) == 8 && sizeof(MS) == 8;
+    StateArr<T, tri(P), kSm> L(lslot);
     T inv[P];
     // smallest pivot ratio d / djj, kept as a fraction (one division at the
     // end instead of one per pivot: FP64 division is long-latency)
@@ -511,11 +530,13 @@ __device__ __noinline__ int chol_solve_fp64(const float *Ms, float par, const fl
 // frame and register spills even when it never runs.
 template <int P, typename T, bool ESC, typename MA>
 __device__ __forceinline__ int damped_solve(const MA &Ms, T par, const T (&g)[P], float thr,
-                                            T (&z)[P], T &znorm, T &w2, T &minpiv, unsigned &n_esc)
+                                            T (&z)[P], T &znorm, T &w2, T &minpiv, unsigned &n_esc,
+                                            T *lslot)
 {
     // FP64 solves take no pivot threshold (there is no higher precision to
     // escalate to), so only FP32 solves can return 1
-    int rc = chol_solve<P, T, T>(Ms, par, g, (ESC && sizeof(T) == 4) ? (T)thr : T(0), z, znorm, w2, minpiv);
+    int rc = chol_solve<P, T, T>(Ms, par, g, (ESC && sizeof(T) == 4) ? (T)thr : T(0), z, znorm, w2, minpiv,
+                                 lslot);
     if constexpr (ESC && sizeof(T) == 4) {
         if (rc == 1) {
             ++n_esc;
@@ -548,7 +569,7 @@ __device__ __forceinline__ int damped_solve(const MA &Ms, T par, const T (&g)[P]
 template <int P, typename T, bool ESC, typename MA>
 __device__ __forceinline__ void lmpar_scaled(const MA &Ms, const T (&g)[P], T delta, T &par,
                                              T (&z)[P], float thr, unsigned &n_lambda, unsigned &n_esc,
-                                             bool &singular, T &newton_piv, T &margin)
+                                             bool &singular, T &newton_piv, T &margin, T *lslot = nullptr)
 {
     const T idelta = frcp(delta);
     T dxnorm, w2, mp;
@@ -566,7 +587,7 @@ __device__ __forceinline__ void lmpar_scaled(const MA &Ms, const T (&g)[P], T de
             pr = t > tiny_pos<T>() ? t : tiny_pos<T>();
         }
         ++n_lambda;
-        const int rc = damped_solve<P, T, ESC>(Ms, pr, g, thr, z, dxnorm, w2, mp, n_esc);
+        const int rc = damped_solve<P, T, ESC>(Ms, pr, g, thr, z, dxnorm, w2, mp, n_esc, lslot);
         if (first) {
             first = false;
             newton_piv = mp;

@@ -294,27 +294,11 @@ template <int P> struct ContLayout {
     static constexpr int STRIDE = ((SC + 11) + 3) / 4 * 4;
 };
 
-// Per-fit array that lives in registers, or (InSmem) in a shared-memory
-// slot of the fit's group; the FP64 solver keeps its normal equations there
-// so that they are not live in registers during the pixel pass.
-template <typename T, int N, bool InSmem> struct StateArr;
-template <typename T, int N> struct StateArr<T, N, false> {
-    T r[N];
-    __device__ __forceinline__ explicit StateArr(T *) {}
-    __device__ __forceinline__ T &operator[](int k) { return r[k]; }
-    __device__ __forceinline__ const T &operator[](int k) const { return r[k]; }
-};
-template <typename T, int N> struct StateArr<T, N, true> {
-    T *p;
-    __device__ __forceinline__ explicit StateArr(T *slot) : p(slot) {}
-    __device__ __forceinline__ T &operator[](int k) { return p[k]; }
-    __device__ __forceinline__ const T &operator[](int k) const { return p[k]; }
-};
 
 // Shared memory of the solver block: the ROIs, then (FP64 only) the
 // per-fit normal equations.
 template <typename T>
-__host__ __device__ constexpr int state_smem_per_fit(int P) { return sizeof(T) == 8 ? (2 * tri(P) + 4 * P) * 8 : 0; }
+__host__ __device__ constexpr int state_smem_per_fit(int P) { return sizeof(T) == 8 ? (3 * tri(P) + 4 * P) * 8 : 0; }
 
 // Process one queue of ROI half-width r: the fresh candidates (level 0) or
 // the fits suspended there (level 1). TPF threads cooperate on each fit;
@@ -603,7 +587,8 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
             unsigned nl = 0, ne = 0;
             bool sing = false;
             T npiv;
-            lmpar_scaled<P, T, ESC>(Ms, g, delta, par, z, a.pivot_thr, nl, ne, sing, npiv, margin_fit);
+            lmpar_scaled<P, T, ESC>(Ms, g, delta, par, z, a.pivot_thr, nl, ne, sing, npiv, margin_fit,
+                                    sstate ? sstate + 2 * NT + 4 * P : nullptr);
             if (leader) {
                 st[ST_LAMBDA] += nl;
                 st[ST_ESC] += ne;
