@@ -175,6 +175,9 @@ typedef struct loc_options {
                                   once (the first scheduling level then runs at
                                   least 4 threads per fit); 0 (default): FP32
                                   throughout */
+    int32_t rerun_capped;      /* 1: fits the FP32 solver stopped at max_iter are
+                                  re-run in FP64 as well; 0: they are kept as
+                                  they are */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */

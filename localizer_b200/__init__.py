@@ -54,7 +54,8 @@ class Options(C.Structure):
                 ("fp64_rerun", C.c_int32), ("rerun_margin", C.c_float), ("rerun_pivot", C.c_float),
                 ("rerun_threads_per_fit", C.c_int32), ("serial_classes", C.c_int32),
                 ("proposal", C.c_void_p), ("warm_iter_limit", C.c_int32), ("long_rerun_iters", C.c_int32),
-                ("long_rerun_threads_per_fit", C.c_int32), ("compensated", C.c_int32)]
+                ("long_rerun_threads_per_fit", C.c_int32), ("compensated", C.c_int32),
+                ("rerun_capped", C.c_int32)]
 
 
 class Stats(C.Structure):

@@ -55,6 +55,7 @@ struct FitParams {
                                     // than long_rerun_iters iterations
     int long_rerun_iters;      // 0: no separate long queue
     int compensated;           // FP32 group sums of the normal equations in FP64 (threads per fit > 1)
+    int rerun_capped;          // also re-run in FP64 the fits FP32 stopped at the iteration cap
     float rerun_margin;        // branch-decision margin below which a fit is flagged
     float rerun_pivot;         // undamped pivot ratio below which a fit is flagged
     const float *init_params;
