@@ -178,6 +178,11 @@ typedef struct loc_options {
     int32_t rerun_capped;      /* 1: fits the FP32 solver stopped at max_iter are
                                   re-run in FP64 as well; 0: they are kept as
                                   they are */
+    float rerun_cond;          /* > 0: a fit is also re-run in FP64 when its
+                                  closest branch margin is below rerun_cond x
+                                  FP32 epsilon / its smallest undamped pivot
+                                  ratio (the FP32 error its conditioning
+                                  allows); 0 (default): off */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */

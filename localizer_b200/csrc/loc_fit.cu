@@ -173,7 +173,8 @@ __global__ void k3_flag(const float *state32, int stride, const int *cls, const 
 template <int P>
 __global__ void k3_flag_class(const float *state32, int stride, const int *order, const int *meta,
                               const uint8_t *flags, int r, float margin, float pivot, int warm_limit, int *cls2,
-                              int *order2, int *meta2, int long_iters, int *order3, int *meta3, int capped)
+                              int *order2, int *meta2, int long_iters, int *order3, int *meta3, int capped,
+                              float cond)
 {
     using SL = StateLayout<P>;
     const int start = meta[m_start(r)], count = meta[m_count(r)];
@@ -191,8 +192,12 @@ __global__ void k3_flag_class(const float *state32, int stride, const int *order
         // capped: fits the FP32 solver stopped at the iteration cap are
         // re-run too (the FP64 solve may converge where FP32 did not)
         const bool is_capped = status == (float)T_MAX_ITER;
+        // cond > 0: a branch margin is also too small when it is within the
+        // FP32 error the fit's conditioning allows (cond * eps32 / smallest
+        // undamped pivot ratio)
+        const float mthr = cond > 0.0f ? fmaxf(margin, cond * 5.96e-8f / fmaxf(s[SL::MINPIV], 1e-30f)) : margin;
         const bool risky = is_capped ? capped != 0
-                                     : (s[SL::MARGIN] < margin || s[SL::MINPIV] < pivot || status != 0.0f ||
+                                     : (s[SL::MARGIN] < mthr || s[SL::MINPIV] < pivot || status != 0.0f ||
                                         (warm_limit > 0 && s[SL::ITERS] > (float)warm_limit));
         if (risky) {
             cls2[i] = r;
@@ -1345,13 +1350,13 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
                 switch (m) {
                 case 0: k3_flag_class<5><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r, p.rerun_margin,
                                                              p.rerun_pivot, wl, s.cls2, s.order2, s.meta2, li, o3,
-                                                             m3, p.rerun_capped); break;
+                                                             m3, p.rerun_capped, p.rerun_cond); break;
                 case 1: k3_flag_class<4><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r, p.rerun_margin,
                                                              p.rerun_pivot, wl, s.cls2, s.order2, s.meta2, li, o3,
-                                                             m3, p.rerun_capped); break;
+                                                             m3, p.rerun_capped, p.rerun_cond); break;
                 default: k3_flag_class<7><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r,
                                                               p.rerun_margin, p.rerun_pivot, wl, s.cls2, s.order2,
-                                                              s.meta2, li, o3, m3, p.rerun_capped); break;
+                                                              s.meta2, li, o3, m3, p.rerun_capped, p.rerun_cond); break;
                 }
                 if ((e = cudaGetLastError()) != cudaSuccess) return e;
                 bump();

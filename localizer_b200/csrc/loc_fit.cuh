@@ -56,6 +56,7 @@ struct FitParams {
     int long_rerun_iters;      // 0: no separate long queue
     int compensated;           // FP32 group sums of the normal equations in FP64 (threads per fit > 1)
     int rerun_capped;          // also re-run in FP64 the fits FP32 stopped at the iteration cap
+    float rerun_cond;          // > 0: margin threshold raised to rerun_cond * eps32 / smallest pivot ratio
     float rerun_margin;        // branch-decision margin below which a fit is flagged
     float rerun_pivot;         // undamped pivot ratio below which a fit is flagged
     const float *init_params;
