@@ -306,7 +306,7 @@ template <int P> struct ContLayout {
 // Shared memory of the solver block: the ROIs, then (FP64 only) the
 // per-fit normal equations.
 template <typename T>
-__host__ __device__ constexpr int state_smem_per_fit(int P) { return sizeof(T) == 8 ? (3 * tri(P) + 4 * P) * 8 : 0; }
+__host__ __device__ constexpr int state_smem_per_fit(int P) { return sizeof(T) == 8 ? (3 * tri(P) + 5 * P) * 8 : 0; }
 
 // Process one queue of ROI half-width r: the fresh candidates (level 0) or
 // the fits suspended there (level 1). TPF threads cooperate on each fit;
@@ -352,7 +352,7 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
     StateArr<T, P, kSmemState> th(sstate ? sstate + NT + P : nullptr);
     StateArr<T, P, kSmemState> D(sstate ? sstate + NT + 2 * P : nullptr);
     StateArr<T, P, kSmemState> dx(sstate ? sstate + NT + 3 * P : nullptr);
-    T te[P];
+    StateArr<T, P, kSmemState> te(sstate ? sstate + 3 * NT + 4 * P : nullptr);
     T fnorm = 0, delta = 0, par = 0, xnorm = 0, jdx2 = 0, pnorm = 0;
     int phase = 0, it_state = 0, iterations = 0, trial = 0, cidx = -1, xo = 0, yo = 0;
     T minpiv_fit = T(1);
@@ -638,10 +638,13 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
         const unsigned pmask = __ballot_sync(kFull, do_pass);
         T acc[NT - 1], vv[P], chi2, dchi, dqmax;
         if (do_pass) {
-            T dt[P];
+            T dt[P], tev[P];
 #pragma unroll
-            for (int k = 0; k < P; ++k) dt[k] = phase == 2 ? dx[k] : T(0);
-            Pass<METHOD, S, TPF, T>::run(myroi, s, q, w0, te, dt, acc, vv, chi2, dchi, dqmax);
+            for (int k = 0; k < P; ++k) {
+                dt[k] = phase == 2 ? dx[k] : T(0);
+                tev[k] = te[k];
+            }
+            Pass<METHOD, S, TPF, T>::run(myroi, s, q, w0, tev, dt, acc, vv, chi2, dchi, dqmax);
             if constexpr (TPF > 1 && sizeof(T) == 4) {
                 if (a.compensated) {
 #pragma unroll
