@@ -183,6 +183,11 @@ typedef struct loc_options {
                                   FP32 epsilon / its smallest undamped pivot
                                   ratio (the FP32 error its conditioning
                                   allows); 0 (default): off */
+    int32_t rerun_iters;       /* > 0: fits whose FP32 solve took at least this
+                                  many iterations are re-run in FP64 as well
+                                  (long, slowly converging fits stop where their
+                                  path takes them under the reference's test_delta);
+                                  0: off */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */
