@@ -395,6 +395,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-next-rows", action="store_true")
     ap.add_argument("--serial-parts", action="store_true", help="the method calls of a step one after the other")
+    ap.add_argument("--warm-study", type=int, default=1,
+                    help="1: add the warm-start study (iteration histograms, re-run limit 8/12/16)")
     ap.add_argument("--train-frames", type=int, default=3000, help="frames whose windows train each proposal")
     ap.add_argument("--train-epochs", type=int, default=8)
     args = ap.parse_args()
@@ -439,6 +441,13 @@ def main():
     if not args.no_warm:
         arm_opts["warm"] = lambda m: L.default_options(max_half_width=mh, precision=args.precision,
                                                        proposal=nets[m].handle.value)
+        if args.warm_study:
+            # the warm-start re-run limit swept: warm fits needing more FP32
+            # iterations than the limit are re-run from the reference start
+            for lim in (12, 16):
+                arm_opts[f"warm_limit{lim}"] = (lambda lim: lambda m: L.default_options(
+                    max_half_width=mh, precision=args.precision, proposal=nets[m].handle.value,
+                    warm_iter_limit=lim))(lim)
     if args.config == 3 and args.precision == 0:
         arm_opts["fp64"] = lambda m: L.default_options(max_half_width=mh, precision=1)
     opts = {arm: {p.method: f(p.method) for p in parts} for arm, f in arm_opts.items()}
@@ -491,7 +500,7 @@ def main():
 
     res = {}
     for arm in opts:
-        res[arm] = timed(arm, args.steps if arm != "fp64" else max(3, args.steps // 4))
+        res[arm] = timed(arm, args.steps if arm in ("plain", "warm") else max(3, args.steps // 4))
         log(f"[bench] arm {arm}: {res[arm]['value'] / 1e6:.2f} M fits/s, {res[arm]['ms'] / args.steps:.1f} ms/step")
     value = res["plain"]["value"]
     elapsed_ms = res["plain"]["ms"]
@@ -672,6 +681,8 @@ def main():
                          "proposal_roofline": prop_roof, "warm_clocks": res["warm"]["clocks"]})
         if "fp64" in res:
             line["precision_report"] = precision_report(res, accuracy, parts)
+        if args.warm_study and "warm" in res:
+            line["warm_study"] = warm_study(L, torch, parts, opts, res, frames_dev, n_frames, size, w, stream)
         print(json.dumps(line))
     for net in nets.values():
         net.close()
@@ -680,6 +691,38 @@ def main():
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def warm_study(L, torch, parts, opts, res, frames_dev, n_frames, size, w, stream):
+    """Cold against warm starts: FP32 iteration histograms of the plain and
+    the warm fits (from the solver's per-fit diagnostics), and, per
+    warm-start re-run limit, the fits/s and the fraction of fits re-run from
+    the reference start."""
+    bins = [1, 2, 3, 4, 5, 6, 7, 8, 10, 12, 16, 20, 32, 64, 201]
+    out = {"iteration_bins": bins, "histogram": {}, "limits": {}}
+    for arm in ("plain", "warm"):
+        hist = np.zeros(len(bins) - 1, dtype=np.int64)
+        for p in parts:
+            dg = torch.zeros((p.n, 8), dtype=torch.float32, device="cuda")
+            o, f = p.out(torch, arm)
+            opt = opts[arm][p.method]
+            saved = opt.d_diag
+            opt.d_diag = dg.data_ptr()
+            p.eng.fit_device(frames_dev.data_ptr(), n_frames, size, size, p.d_cands.data_ptr(), p.n, p.method, w.w0,
+                             1.0, o.data_ptr(), f.data_ptr(), stream.cuda_stream, opt)
+            p.eng.sync(stream.cuda_stream)
+            opt.d_diag = saved
+            it = dg[:, 5].cpu().numpy()
+            hist += np.histogram(it[it > 0], bins=bins)[0]
+        out["histogram"][arm] = hist.tolist()
+    for arm, lim in (("warm", 8), ("warm_limit12", 12), ("warm_limit16", 16)):
+        if arm not in res:
+            continue
+        s = res[arm]["stats"]
+        out["limits"][str(lim)] = {"fits_per_s": res[arm]["value"],
+                                   "rerun_fraction": sum(v["fits_fp64_rerun"] for v in s.values()) /
+                                   max(sum(v["fits"] for v in s.values()), 1)}
+    return out
 
 
 def precision_report(res, accuracy, parts):
