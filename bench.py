@@ -263,10 +263,12 @@ def calibrate_per_fit(frames_host, cands, methods, w0):
     return max((time.perf_counter() - t) / max(len(sel), 1), 1e-6)
 
 
-def accuracy_report(rows, flags, ref_rows, ref_kept, ref_iters, method):
+def accuracy_report(rows, flags, ref_rows, ref_kept, ref_iters, method, rows64=None, flags64=None):
     """Flag agreement and position error against the reference fitter, with
     the tail split by class: fits the reference stopped at its 200-iteration
-    cap (not converged) and fits it converged."""
+    cap (not converged) and fits it converged; among the converged ones
+    beyond 1e-3 px, those the GPU's all-FP64 solve also misses
+    (rounding-sensitive) and those only this path misses."""
     gk = flags == 0
     xi = XCOL[method]
     both = gk & ref_kept
@@ -279,6 +281,17 @@ def accuracy_report(rows, flags, ref_rows, ref_kept, ref_iters, method):
             rep[name] = {"n": int(cls.sum()), "position_within_1e-3px": float(np.mean(err < 1e-3)),
                          "n_beyond_1e-3px": int(np.sum(err >= 1e-3)), "position_max_err_px": float(err.max()),
                          "position_rms_err_px": float(np.sqrt(np.mean(err ** 2)))}
+            if rows64 is not None and name == "converged":
+                idx = np.nonzero(cls)[0]
+                k64 = flags64[idx] == 0
+                e64 = np.abs(rows64[idx, xi:xi + 2] - ref_rows[idx, xi:xi + 2]).max(axis=1)
+                miss = err >= 1e-3
+                rs = miss & (~k64 | (e64 >= 1e-3))
+                only = miss & ~rs
+                rep[name]["rounding_sensitive"] = int(rs.sum())
+                rep[name]["fp32_only"] = int(only.sum())
+                rep[name]["fp32_only_max_err_px"] = float(err[only].max()) if only.any() else 0.0
+                rep[name]["fp64_gpu_within_1e-3px"] = float(np.mean(k64 & (e64 < 1e-3)))
         else:
             rep[name] = {"n": 0}
     return rep
@@ -617,7 +630,22 @@ def main():
             cpu = {"value": len(sel) / dt, "unit": UNIT, "cores": th, "kind": "reference",
                    "sample": f"{len(sel)} candidates of {len(chosen)} whole frames spread through the stack; "
                              f"reference Localization.cpp FP64 + lmsder restatement, {th} host threads"}
-            accuracy = {"sample_fits": int(len(sel)), "reference": "reference fitter (FP64) on the same candidates"}
+            accuracy = {"sample_fits": int(len(sel)), "reference": "reference fitter (FP64) on the same candidates",
+                        "classes": "converged fits beyond 1e-3 px: rounding_sensitive (the GPU's all-FP64 solve "
+                                   "misses too) or fp32_only"}
+            # the sample's candidates once more, all in FP64 on the GPU
+            fp64 = {}
+            for p in parts:
+                idx_s = ref[p.method][0]
+                sub = np.ascontiguousarray(cands[sel[idx_s]])
+                d_sub = torch.from_numpy(sub.view(np.uint8)).cuda()
+                o64 = torch.empty((len(sub), p.ncol), dtype=torch.float64, device="cuda")
+                f64 = torch.empty(len(sub), dtype=torch.uint8, device="cuda")
+                p.eng.fit_device(frames_dev.data_ptr(), n_frames, size, size, d_sub.data_ptr(), len(sub), p.method,
+                                 w.w0, 1.0, o64.data_ptr(), f64.data_ptr(), stream.cuda_stream,
+                                 L.default_options(max_half_width=mh, precision=1))
+                p.eng.sync(stream.cuda_stream)
+                fp64[p.method] = (o64.cpu().numpy(), f64.cpu().numpy())
             for arm in res:
                 accuracy[arm] = {}
                 for p in parts:
@@ -627,7 +655,8 @@ def main():
                     o, f = p.out(torch, arm)
                     t = torch.from_numpy(pos).cuda()
                     accuracy[arm][f"method_{p.method}"] = accuracy_report(o[t].cpu().numpy(), f[t].cpu().numpy(),
-                                                                          rrows, rkept, rit, p.method)
+                                                                          rrows, rkept, rit, p.method,
+                                                                          *fp64[p.method])
 
     next_rows = None
     if rank == 0 and not args.no_next_rows:

@@ -128,7 +128,8 @@ typedef struct loc_options {
                                   re-run in FP64, iterations and status of the
                                   FP32 run, reserved */
     int32_t threads_per_fit;   /* threads cooperating on one fit in the first
-                                  scheduling level: 1 (default), 4 or 8 */
+                                  scheduling level: 1 (default), 4, 8, 16 or 32
+                                  (a warp per fit) */
     int32_t tail_threads_per_fit; /* threads per fit for fits that outlive the
                                   first level's budget: 8 (default), 4 or 1 */
     int32_t level0_budget;     /* solver iterations a fit may use in the first
@@ -139,8 +140,9 @@ typedef struct loc_options {
                                   depend on FP32 rounding are re-run entirely in
                                   FP64 on the GPU (a solver branch decision within
                                   rerun_margin of its threshold, an undamped pivot
-                                  ratio below rerun_pivot, or a stop for lack of
-                                  progress; fits that reach max_iter are not);
+                                  ratio below rerun_pivot, a stop for lack of
+                                  progress, or at least rerun_iters iterations;
+                                  fits that reach max_iter only with rerun_capped);
                                   -1: never */
     float rerun_margin;        /* 0: default 1e-4 */
     float rerun_pivot;         /* 0: default 1e-4 */
@@ -183,11 +185,12 @@ typedef struct loc_options {
                                   FP32 epsilon / its smallest undamped pivot
                                   ratio (the FP32 error its conditioning
                                   allows); 0 (default): off */
-    int32_t rerun_iters;       /* > 0: fits whose FP32 solve took at least this
-                                  many iterations are re-run in FP64 as well
-                                  (long, slowly converging fits stop where their
-                                  path takes them under the reference's test_delta);
-                                  0: off */
+    int32_t rerun_iters;       /* fits whose FP32 solve took at least this many
+                                  iterations are re-run in FP64 as well (long,
+                                  slowly converging fits stop where their path
+                                  takes them under the reference's test_delta, so
+                                  FP32 rounding moves their end point); 0: default
+                                  16; < 0: off */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */

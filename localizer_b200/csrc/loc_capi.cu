@@ -281,7 +281,7 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     p.compensated = o.compensated > 0 ? 1 : 0;
     p.rerun_capped = o.rerun_capped > 0 ? 1 : 0;
     p.rerun_cond = o.rerun_cond > 0 ? o.rerun_cond : 0.0f;
-    p.rerun_iters = o.rerun_iters > 0 ? o.rerun_iters : 0;
+    p.rerun_iters = o.rerun_iters == 0 ? 16 : (o.rerun_iters < 0 ? 0 : o.rerun_iters);
     p.rerun_margin = o.rerun_margin > 0 ? o.rerun_margin : 1e-4f;
     p.rerun_pivot = o.rerun_pivot > 0 ? o.rerun_pivot : 1e-4f;
     p.long_rerun_threads_per_fit = o.long_rerun_threads_per_fit > 0 ? o.long_rerun_threads_per_fit : 8;
@@ -290,9 +290,10 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     if (!(p.long_rerun_threads_per_fit == 1 || p.long_rerun_threads_per_fit == 2 ||
           p.long_rerun_threads_per_fit == 4 || p.long_rerun_threads_per_fit == 8))
         return fail(LOC_E_INVALID, "long_rerun_threads_per_fit must be 1, 2, 4 or 8");
-    if (!(p.threads_per_fit == 1 || p.threads_per_fit == 4 || p.threads_per_fit == 8) ||
+    if (!(p.threads_per_fit == 1 || p.threads_per_fit == 4 || p.threads_per_fit == 8 || p.threads_per_fit == 16 ||
+          p.threads_per_fit == 32) ||
         !(p.tail_threads_per_fit == 1 || p.tail_threads_per_fit == 4 || p.tail_threads_per_fit == 8))
-        return fail(LOC_E_INVALID, "threads per fit must be 1, 4 or 8");
+        return fail(LOC_E_INVALID, "threads per fit must be 1, 4, 8, 16 or 32 (second level: 1, 4 or 8)");
     p.init_params = o.d_init_params;
     p.warm = warm;
     p.prop = prop;

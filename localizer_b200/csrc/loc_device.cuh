@@ -227,6 +227,17 @@ __device__ __forceinline__ void pass_sym(const float *__restrict__ roi, int ld, 
         vv[3] = fma(jy, r, vv[3]); vv[4] += r;
         chi2 = fma(r, r, chi2);
     };
+    if constexpr (TPF >= 16) {
+        // a half or whole warp per fit: the flattened ROI is dealt out over
+        // the lanes (row-wise dealing would idle the lanes past a row's end)
+#pragma unroll 1
+        for (int k = q; k < s * s; k += TPF) {
+            const int j = k / s, i = k - j * s;
+            const T wy = (T)j - y0;
+            body(i, wy, wy * wy, -dxs * dxs - dys * (T(2) * wy + dys), roi + j * s * ld);
+        }
+        return;
+    }
 #pragma unroll 1
     for (int j = 0; j < s; ++j) {
         const T wy = (T)j - y0;
@@ -287,6 +298,15 @@ __device__ __forceinline__ void pass_fixed(const float *__restrict__ roi, int ld
         vv[0] = fma(e, r, vv[0]); vv[1] = fma(jx, r, vv[1]); vv[2] = fma(jy, r, vv[2]); vv[3] += r;
         chi2 = fma(r, r, chi2);
     };
+    if constexpr (TPF >= 16) {
+#pragma unroll 1
+        for (int k = q; k < s * s; k += TPF) {
+            const int j = k / s, i = k - j * s;
+            const T wy = (T)j - y0;
+            body(i, wy, wy * wy, -dxs * dxs - dys * (T(2) * wy + dys), roi + j * s * ld);
+        }
+        return;
+    }
 #pragma unroll 1
     for (int j = 0; j < s; ++j) {
         const T wy = (T)j - y0;
@@ -381,6 +401,25 @@ __device__ __forceinline__ void pass_ell(const float *__restrict__ roi, int ld, 
         vv[6] += r;
         chi2 = fma(r, r, chi2);
     };
+    auto row_terms = [&](int j, T &wy, T &wy2, T &wc, T &wrb, T &brow, T &crow) {
+        wy = (T)j - y0;
+        wy2 = wy * wy;
+        wc = wy * c;
+        wrb = wy * rb;
+        const T wcur = wy + dys;
+        brow = T(2) * (dxs * (da - a) - drb * wy + rb0 * dys);
+        crow = (da - a) * dx2 - c * dys * (T(2) * wy + dys) + dcq * wcur * wcur + T(2) * rb0 * dxs * wcur;
+    };
+    if constexpr (TPF >= 16) {
+#pragma unroll 1
+        for (int k = q; k < s * s; k += TPF) {
+            const int j = k / s, i = k - j * s;
+            T wy, wy2, wc, wrb, brow, crow;
+            row_terms(j, wy, wy2, wc, wrb, brow, crow);
+            body(i, wy, wy2, wc, wrb, brow, crow, roi + j * s * ld);
+        }
+        return;
+    }
 #pragma unroll 1
     for (int j = 0; j < s; ++j) {
         const T wy = (T)j - y0;

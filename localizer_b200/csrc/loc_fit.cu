@@ -1135,6 +1135,9 @@ cudaError_t launch_k1(const K1Args &ka, int r, int tpb, int bps_req, int tpf, cu
         switch (tpf) {
         case 4: return launch_k1_tpf<METHOD, T, 4>(ka, r, tpb, bps_req, stream);
         case 8: return launch_k1_tpf<METHOD, T, 8>(ka, r, tpb, bps_req, stream);
+        // a half warp or a whole warp per fit (runtime ROI side only)
+        case 16: return launch_k1_s<METHOD, T, 0, 16>(ka, r, tpb, bps_req, stream);
+        case 32: return launch_k1_s<METHOD, T, 0, 32>(ka, r, tpb, bps_req, stream);
         default: return launch_k1_tpf<METHOD, T, 1>(ka, r, tpb, bps_req, stream);
         }
     }

@@ -7,6 +7,8 @@ reference's own fitter on the same particle lists; and the reference-DLL
 entry point LocalizerFitEmitters (source/LocalizerDLL.cpp:89-129) against
 the reference pipeline it replaces (GLRT + adjacent-8 +
 FitPositions_EllipsoidalGaussian(psfWidth, 1.0))."""
+import os
+
 import numpy as np
 import pytest
 
@@ -15,6 +17,7 @@ from oracle import oracle as O
 from tests import _golden as G
 
 pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 XCOL = {0: 3, 1: 2, 5: 4, 6: 3, 7: 4}
 
@@ -23,12 +26,29 @@ def _index(cands):
     return {(int(c["frame"]), float(c["x"]), float(c["y"])): k for k, c in enumerate(cands)}
 
 
+def _compare_in_child(name, method, tmp_path):
+    """Run the adapter and the reference fitter in a child process (a fault
+    in either then fails this test with its stderr instead of ending the
+    session) and load both results."""
+    import subprocess
+    import sys
+    out = tmp_path / "cmp.npz"
+    code = ("import sys, numpy as np; sys.path.insert(0, {root!r}); "
+            "from oracle import oracle as O; from tests import _golden as G; "
+            "g = G.load({name!r}); r = O.capi_compare(g['frames'], g['cands'], {method}, g['w0']); "
+            "np.savez({out!r}, **r)").format(root=ROOT, name=name, method=method, out=str(out))
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-3000:]
+    z = np.load(out)
+    return {k: z[k] for k in z.files}
+
+
 @pytest.mark.skipif(not O.capi_available(), reason="adapter library not built (needs the reference tree)")
 @pytest.mark.parametrize("name,method", list(G.all_cases()))
-def test_fitpositions_gpu_adapter_matches_reference_fitter(name, method):
+def test_fitpositions_gpu_adapter_matches_reference_fitter(name, method, tmp_path):
     g = G.load(name)
     cands = g["cands"]
-    r = O.capi_compare(g["frames"], cands, method, g["w0"])
+    r = _compare_in_child(name, method, tmp_path)
     gm, rm, gl, rl = r["gpu_matrix"], r["ref_matrix"], r["gpu_left"], r["ref_left"]
     # one container row per particle left in the list, on both sides
     assert len(gm) == len(gl) and len(rm) == len(rl)

@@ -12,7 +12,8 @@ checked through properties that do not depend on its size:
 * the solver fitted exactly the candidates that the edge rule kept;
 * a fit does not depend on the batch around it: the candidates of a sample
   of frames fitted as a small batch give bit-identical rows and flags;
-* on that sample the FP64 oracle's gates hold (flags, positions <= 1e-3 px).
+* on that sample the FP64 oracle's gates hold (flags; positions <= 1e-3 px
+  except the named classes of tests/test_gpu_parity.py, bounded by count).
 """
 import numpy as np
 import pytest
@@ -20,6 +21,7 @@ import pytest
 import localizer_b200 as L
 from localizer_b200 import synth
 from oracle import oracle as O
+from tests.test_gpu_parity import check_classes, parity_classes
 
 pytestmark = pytest.mark.gpu
 
@@ -28,7 +30,7 @@ FINITE_COLS = {0: [0, 1, 2, 3, 4, 5], 7: [0, 4, 5, 6, 7]}   # always finite in k
 SAMPLE_FRAMES = 40
 
 
-def _fit(engine, d_frames, cands, method, w0):
+def _fit(engine, d_frames, cands, method, w0, precision=0):
     import torch
     n = len(cands)
     ncol = L.lib().loc_output_columns(method)
@@ -38,7 +40,7 @@ def _fit(engine, d_frames, cands, method, w0):
     stream = torch.cuda.current_stream().cuda_stream
     engine.fit_device(d_frames.data_ptr(), d_frames.shape[0], d_frames.shape[2], d_frames.shape[1], d_c.data_ptr(),
                       n, method, w0, 1.0, d_o.data_ptr(), d_f.data_ptr(), stream,
-                      L.default_options(max_half_width=int(cands["half_width"].max())))
+                      L.default_options(max_half_width=int(cands["half_width"].max()), precision=precision))
     engine.sync(stream)
     return d_c, d_o, d_f
 
@@ -106,7 +108,8 @@ def test_dense_workload_full_size():
         gkept = flags_full == 0
         capped = out[:, ref + 1] == 1
         assert np.sum(gkept != okept) <= max(1, int(0.001 * len(sub))), np.mean(gkept == okept)
-        both = gkept & okept & ~capped
-        err = np.abs(rows_full[both, xi:xi + 2] - out[both, xi:xi + 2]).max(axis=1)
-        assert np.mean(err < 1e-3) >= 0.999 or np.sum(err >= 1e-3) <= 1, np.sort(err)[-5:]
+        # the same fits in FP64 on the GPU name the rounding-sensitive ones
+        _, o64, f64 = _fit(engine, d_frames, part[sel], method, w.w0, precision=1)
+        check_classes(parity_classes(rows_full, flags_full, o64.cpu().numpy(), f64.cpu().numpy(), out, okept, ~capped,
+                                     method))
     engine.close()

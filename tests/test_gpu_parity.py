@@ -8,6 +8,18 @@ Fits that reach the 200-iteration cap in the FP64 reference (termination
 status 1) have not converged: their final point depends on every rounding
 of a long wandering trajectory, so they count for flag agreement but not
 for the position gate; the tests assert that they are rare.
+
+Every converged, jointly kept fit is in one of three classes:
+* within 1e-3 px of the reference;
+* rounding-sensitive: the GPU's all-FP64 solve of the same fit also ends
+  1e-3 px or more away (normal equations and Cholesky in place of the
+  reference's QR change roundings at the 1e-16 level, and these fits'
+  end points follow them: a slow approach under the reference's loose
+  test_delta, or a path that leaves for another minimum);
+* FP32-only: the FP32 path misses while the FP64 solve does not.
+The last two are bounded by count (RS_FRACTION, FP32_ONLY_FRACTION of the
+converged fits, at least one each), not by size: a fit that follows a
+different path can end pixels away.
 """
 import numpy as np
 import pytest
@@ -20,8 +32,10 @@ from tests import _golden as G
 pytestmark = pytest.mark.gpu
 
 POS_TOL = 1e-3            # px, FP32 path vs FP64 oracle
-POS_FRACTION = 0.999      # fraction of jointly kept rows within POS_TOL
+POS_FRACTION = 0.9995     # fraction of jointly kept, converged rows within POS_TOL
 FLAG_AGREEMENT = 0.999
+RS_FRACTION = 5e-4        # rounding-sensitive fits (the FP64 GPU solve misses too)
+FP32_ONLY_FRACTION = 1e-4 # fits only the FP32 path misses
 POS_TOL_FP64 = 1e-6       # px, FP64 GPU path vs FP64 oracle
 XCOL = {0: 3, 1: 2, 5: 4, 7: 4}
 
@@ -31,6 +45,27 @@ def engine():
     e = L.Engine(0)
     yield e
     e.close()
+
+
+def parity_classes(rows, flags, rows64, flags64, ref_rows, ref_kept, ref_converged, method):
+    """Counts of the three classes over the converged fits kept by the
+    reference, the FP32 path and the FP64 path."""
+    xi = XCOL[method]
+    both = (flags == 0) & (flags64 == 0) & ref_kept & ref_converged
+    e32 = np.abs(rows[both, xi:xi + 2] - ref_rows[both, xi:xi + 2]).max(axis=1)
+    e64 = np.abs(rows64[both, xi:xi + 2] - ref_rows[both, xi:xi + 2]).max(axis=1)
+    rs = e64 >= POS_TOL
+    only = (e32 >= POS_TOL) & ~rs
+    return {"n": int(both.sum()), "within": float(np.mean(e32 < POS_TOL)) if both.any() else 1.0,
+            "rounding_sensitive": int(rs.sum()), "fp32_only": int(only.sum()),
+            "fp32_only_max_err": float(e32[only].max()) if only.any() else 0.0}
+
+
+def check_classes(c):
+    n = max(c["n"], 1)
+    assert c["within"] >= POS_FRACTION or c["n"] - int(round(c["within"] * c["n"])) <= 2, c
+    assert c["rounding_sensitive"] <= max(1, int(RS_FRACTION * n)), c
+    assert c["fp32_only"] <= max(1, int(FP32_ONLY_FRACTION * n)), c
 
 
 def compare(rows, flags, ref_rows, ref_kept, method, ref_converged=None):
@@ -49,14 +84,16 @@ def compare(rows, flags, ref_rows, ref_kept, method, ref_converged=None):
 def test_fp32_matches_reference_golden(engine, name, method):
     g = G.load(name)
     rows, flags = engine.fit_host(g["frames"], g["cands"], method, g["w0"])
+    rows64, flags64 = engine.fit_host(g["frames"], g["cands"], method, g["w0"], options=L.default_options(precision=1))
     ref_kept = g[f"kept_{method}"] == 1
     capped = g[f"iters_{method}"] >= 200
     assert np.mean(capped) < 0.03
-    agree, frac, err, both = compare(rows, flags, g[f"out_{method}"], ref_kept, method, ~capped)
     n = len(flags)
     # small fixtures: at most one disagreement where 0.1 % of n is below one
-    assert np.sum((flags == 0) != ref_kept) <= max(1, int(0.001 * n)), (agree, np.nonzero((flags == 0) != ref_kept))
-    assert np.sum(err >= POS_TOL) <= max(1, int((1 - POS_FRACTION) * len(err))), np.sort(err)[-5:]
+    assert np.sum((flags == 0) != ref_kept) <= max(1, int(0.001 * n)), np.nonzero((flags == 0) != ref_kept)
+    c = parity_classes(rows, flags, rows64, flags64, g[f"out_{method}"], ref_kept, ~capped, method)
+    # the fixtures hold no rounding-sensitive fit and no FP32-only miss
+    assert c["rounding_sensitive"] == 0 and c["fp32_only"] == 0, c
     # edge rejects are decided before any arithmetic: exact
     assert np.array_equal(flags == 1, np.isnan(g[f"out_{method}"][:, 1]) & (g[f"iters_{method}"] < 0))
 
@@ -90,13 +127,14 @@ def _workload(name, n_frames, seed=None):
 def test_fp32_matches_oracle_seeded(engine, wname, method, n_frames):
     w, frames, cands = _workload(wname, n_frames)
     rows, flags = engine.fit_host(frames, cands, method, w.w0)
+    rows64, flags64 = engine.fit_host(frames, cands, method, w.w0, options=L.default_options(precision=1))
     out, oflags, _, _ = O.fit(frames, cands, method, w.w0, nthreads=8)
     ncol = O.REF_COLUMNS[method]
     capped = out[:, ncol + 1] == 1
     assert np.mean(capped) < 0.02
     agree, frac, err, both = compare(rows, flags, out, oflags == 0, method, ~capped)
     assert agree >= FLAG_AGREEMENT or np.sum((flags == 0) != (oflags == 0)) <= 1, agree
-    assert frac >= POS_FRACTION or np.sum(err >= POS_TOL) <= 1, (frac, np.sort(err)[-5:])
+    check_classes(parity_classes(rows, flags, rows64, flags64, out, oflags == 0, ~capped, method))
     # widths / background / integral: relative 1e-3; uncertainties: 1e-2
     value_cols = {0: [1, 2, 5], 1: [1, 4], 5: [1, 2, 3, 7], 7: [1, 2, 3, 7]}[method]
     dev_cols = {0: [6, 7, 8, 9, 10], 1: [5, 6, 7, 8], 5: [11, 12, 14], 7: [11, 12, 14]}[method]
