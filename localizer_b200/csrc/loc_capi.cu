@@ -436,10 +436,10 @@ LOC_API int loc_autotune(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, i
     // default shape's results
     const std::vector<std::pair<int loc_ctx::Shape::*, std::vector<int>>> knobs = {
         {&loc_ctx::Shape::tpb, {128, 96, 64}},
-        {&loc_ctx::Shape::tpf, {1, 4, 8}},
+        {&loc_ctx::Shape::tpf, {1, 4, 8, 16, 32}},
         {&loc_ctx::Shape::budget, {16, 24, 32, 48, 64}},
         {&loc_ctx::Shape::tail_tpf, {8, 4}},
-        {&loc_ctx::Shape::rerun_tpf, {2, 1, 4}},
+        {&loc_ctx::Shape::rerun_tpf, {2, 1, 4, 8}},
         {&loc_ctx::Shape::long_tpf, {8, 4, 2}},
     };
     for (size_t kk = 0; rc == LOC_OK && kk < knobs.size(); ++kk) {

@@ -48,9 +48,9 @@ def test_tuned_shape_is_applied_and_keeps_results(method):
         base = L.default_options(max_half_width=6)
         t = eng.autotune(frames.data_ptr(), frames.shape[0], frames.shape[2], frames.shape[1], d_cands.data_ptr(),
                          n, method, w.w0, options=base)
-        assert t["threads_per_fit"] in (1, 4, 8) and t["tail_threads_per_fit"] in (4, 8)
+        assert t["threads_per_fit"] in (1, 4, 8, 16, 32) and t["tail_threads_per_fit"] in (4, 8)
         assert t["level0_budget"] in (16, 24, 32, 48, 64) and t["threads_per_block"] in (64, 96, 128)
-        assert t["rerun_threads_per_fit"] in (1, 2, 4) and t["long_rerun_threads_per_fit"] in (2, 4, 8)
+        assert t["rerun_threads_per_fit"] in (1, 2, 4, 8) and t["long_rerun_threads_per_fit"] in (2, 4, 8)
         assert t["trials"] >= 10 and 0 < t["ms_tuned"] <= t["ms_default"]
         lim = max(1, n // 10000)
         assert t["flag_changes"] <= lim and t["position_changes"] <= lim
