@@ -408,6 +408,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-next-rows", action="store_true")
     ap.add_argument("--serial-parts", action="store_true", help="the method calls of a step one after the other")
+    ap.add_argument("--rerun-iters", type=int, default=0,
+                    help="plain arm: FP64 re-run of fits with at least this many FP32 iterations (0: library "
+                         "default, < 0: off)")
     ap.add_argument("--warm-study", type=int, default=1,
                     help="1: add the warm-start study (iteration histograms, re-run limit 8/12/16)")
     ap.add_argument("--train-frames", type=int, default=3000, help="frames whose windows train each proposal")
@@ -450,7 +453,8 @@ def main():
             nets[p.method], train_rep[p.method] = net, rep
             log(f"[bench] proposal for method {p.method} trained in {rep['wall_s']:.1f}s ({rep['labelled']} windows, "
                 f"holdout position median {rep['holdout_pos_median_px']:.3f} px)")
-    arm_opts = {"plain": lambda m: L.default_options(max_half_width=mh, precision=args.precision)}
+    arm_opts = {"plain": lambda m: L.default_options(max_half_width=mh, precision=args.precision,
+                                                     rerun_iters=args.rerun_iters)}
     if not args.no_warm:
         arm_opts["warm"] = lambda m: L.default_options(max_half_width=mh, precision=args.precision,
                                                        proposal=nets[m].handle.value)
@@ -613,7 +617,9 @@ def main():
             o, f = p.out(torch, "plain")
             sel = torch.from_numpy(pos).cuda()
             assert np.array_equal(pf.numpy(), f[sel].cpu().numpy())
-            assert np.array_equal(po.numpy()[:, :-2], o[sel].cpu().numpy()[:, :-2], equal_nan=True)
+            # the block's calls number frames from the block's first frame
+            assert np.array_equal(po.numpy()[:, 0] + b0, o[sel].cpu().numpy()[:, 0])
+            assert np.array_equal(po.numpy()[:, 1:-2], o[sel].cpu().numpy()[:, 1:-2], equal_nan=True)
         log(f"[bench] e2e: {e_rate / 1e6:.2f} M fits/s")
 
     # CPU reference on a bounded sample of whole frames, and the accuracy of
