@@ -69,7 +69,7 @@ XCOL = {0: 3, 1: 2, 5: 4, 7: 4}
 # DRAM bytes per fit of the whole plain-arm solver chain (every kernel of the
 # step) from an ncu capture, or None while no capture of the current kernels
 # exists
-TRAFFIC_PER_FIT = None
+TRAFFIC_PER_FIT = {"bytes": 1925.0, "source": "profiles/launches_dense500_plain.md (dense workload, 500 frames)"}
 
 CONFIGS = {
     1: {"workload": "small", "block": 0,
