@@ -191,6 +191,10 @@ typedef struct loc_options {
                                   takes them under the reference's test_delta, so
                                   FP32 rounding moves their end point); 0: default
                                   16; < 0: off */
+    float rerun_lastr;         /* > 0: the rerun_iters rule applies only to fits
+                                  whose last step was at least this fraction of
+                                  the test_delta tolerance (a slow approach to
+                                  the stopping test); 0: every long fit */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */

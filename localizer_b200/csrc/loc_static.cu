@@ -153,6 +153,7 @@ extern "C" LOC_API int loc_fit_batch_static(const uint16_t *d_frames, int n_fram
     p.rerun_capped = o.rerun_capped > 0 ? 1 : 0;
     p.rerun_cond = o.rerun_cond > 0 ? o.rerun_cond : 0.0f;
     p.rerun_iters = o.rerun_iters == 0 ? 16 : (o.rerun_iters < 0 ? 0 : o.rerun_iters);
+    p.rerun_lastr = o.rerun_lastr > 0 ? o.rerun_lastr : 0.0f;
     p.rerun_margin = o.rerun_margin > 0 ? o.rerun_margin : 1e-4f;
     p.rerun_pivot = o.rerun_pivot > 0 ? o.rerun_pivot : 1e-4f;
     p.init_params = o.d_init_params;
