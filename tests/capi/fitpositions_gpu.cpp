@@ -58,8 +58,16 @@ public:
         if (n > 0 && loc_fit_host(ctx, frame.data(), 1, nRows, nCols, cands.data(), n, method, w0, sigma, &opt,
                                   rows.data(), flags.data()) != LOC_OK)
             throw std::runtime_error(loc_last_error());
+        // erase the rejects from the caller's list as the reference's fitters
+        // do; the symmetric-PSF filter of method 5 drops positions from the
+        // container but leaves their particles in the list
+        // (Localization.cpp:606-631)
         auto it = particles->begin();
-        for (int k = 0; k < n; ++k) it = flags[k] ? particles->erase(it) : std::next(it);
+        for (int k = 0; k < n; ++k) {
+            const bool erase = flags[k] != LOC_FLAG_KEPT && flags[k] != LOC_FLAG_SYMPSF_RATIO &&
+                               flags[k] != LOC_FLAG_SYMPSF_WIDTH;
+            it = erase ? particles->erase(it) : std::next(it);
+        }
         return makeContainer(rows, flags, ncol);
     }
 
