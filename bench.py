@@ -408,9 +408,6 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-next-rows", action="store_true")
     ap.add_argument("--serial-parts", action="store_true", help="the method calls of a step one after the other")
-    ap.add_argument("--rerun-lastr", type=float, default=0.0,
-                    help="plain arm: the iteration re-run rule only for fits whose last step was at least this "
-                         "fraction of the stopping tolerance")
     ap.add_argument("--rerun-iters", type=int, default=0,
                     help="plain arm: FP64 re-run of fits with at least this many FP32 iterations (0: library "
                          "default, < 0: off)")
@@ -457,7 +454,7 @@ def main():
             log(f"[bench] proposal for method {p.method} trained in {rep['wall_s']:.1f}s ({rep['labelled']} windows, "
                 f"holdout position median {rep['holdout_pos_median_px']:.3f} px)")
     arm_opts = {"plain": lambda m: L.default_options(max_half_width=mh, precision=args.precision,
-                                                     rerun_iters=args.rerun_iters, rerun_lastr=args.rerun_lastr)}
+                                                     rerun_iters=args.rerun_iters)}
     if not args.no_warm:
         arm_opts["warm"] = lambda m: L.default_options(max_half_width=mh, precision=args.precision,
                                                        proposal=nets[m].handle.value)

@@ -189,12 +189,9 @@ typedef struct loc_options {
                                   iterations are re-run in FP64 as well (long,
                                   slowly converging fits stop where their path
                                   takes them under the reference's test_delta, so
-                                  FP32 rounding moves their end point); 0: default
-                                  16; < 0: off */
-    float rerun_lastr;         /* > 0: the rerun_iters rule applies only to fits
-                                  whose last step was at least this fraction of
-                                  the test_delta tolerance (a slow approach to
-                                  the stopping test); 0: every long fit */
+                                  FP32 rounding moves their end point); 0: default,
+                                  16 for the ellipsoidal methods 5 and 7, off for
+                                  methods 0 and 1; < 0: off */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */

@@ -174,7 +174,7 @@ template <int P>
 __global__ void k3_flag_class(const float *state32, int stride, const int *order, const int *meta,
                               const uint8_t *flags, int r, float margin, float pivot, int warm_limit, int *cls2,
                               int *order2, int *meta2, int long_iters, int *order3, int *meta3, int capped,
-                              float cond, int iters_min, float lastr_min)
+                              float cond, int iters_min)
 {
     using SL = StateLayout<P>;
     const int start = meta[m_start(r)], count = meta[m_count(r)];
@@ -199,8 +199,7 @@ __global__ void k3_flag_class(const float *state32, int stride, const int *order
         const bool risky = is_capped ? capped != 0
                                      : (s[SL::MARGIN] < mthr || s[SL::MINPIV] < pivot || status != 0.0f ||
                                         (warm_limit > 0 && s[SL::ITERS] > (float)warm_limit) ||
-                                        (iters_min > 0 && s[SL::ITERS] >= (float)iters_min &&
-                                         s[SL::LASTR] >= lastr_min));
+                                        (iters_min > 0 && s[SL::ITERS] >= (float)iters_min));
         if (risky) {
             cls2[i] = r;
             if (meta3 && s[SL::ITERS] > (float)long_iters) {
@@ -1360,13 +1359,13 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
                 switch (m) {
                 case 0: k3_flag_class<5><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r, p.rerun_margin,
                                                              p.rerun_pivot, wl, s.cls2, s.order2, s.meta2, li, o3,
-                                                             m3, p.rerun_capped, p.rerun_cond, p.rerun_iters, p.rerun_lastr); break;
+                                                             m3, p.rerun_capped, p.rerun_cond, p.rerun_iters); break;
                 case 1: k3_flag_class<4><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r, p.rerun_margin,
                                                              p.rerun_pivot, wl, s.cls2, s.order2, s.meta2, li, o3,
-                                                             m3, p.rerun_capped, p.rerun_cond, p.rerun_iters, p.rerun_lastr); break;
+                                                             m3, p.rerun_capped, p.rerun_cond, p.rerun_iters); break;
                 default: k3_flag_class<7><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r,
                                                               p.rerun_margin, p.rerun_pivot, wl, s.cls2, s.order2,
-                                                              s.meta2, li, o3, m3, p.rerun_capped, p.rerun_cond, p.rerun_iters, p.rerun_lastr); break;
+                                                              s.meta2, li, o3, m3, p.rerun_capped, p.rerun_cond, p.rerun_iters); break;
                 }
                 if ((e = cudaGetLastError()) != cudaSuccess) return e;
                 bump();

@@ -152,8 +152,10 @@ extern "C" LOC_API int loc_fit_batch_static(const uint16_t *d_frames, int n_fram
     p.compensated = o.compensated > 0 ? 1 : 0;
     p.rerun_capped = o.rerun_capped > 0 ? 1 : 0;
     p.rerun_cond = o.rerun_cond > 0 ? o.rerun_cond : 0.0f;
-    p.rerun_iters = o.rerun_iters == 0 ? 16 : (o.rerun_iters < 0 ? 0 : o.rerun_iters);
-    p.rerun_lastr = o.rerun_lastr > 0 ? o.rerun_lastr : 0.0f;
+    // default: the iteration rule for the ellipsoidal fits only (symmetric
+    // and fixed-width fits keep their FP32 end points to 1e-3 px without it)
+    p.rerun_iters = o.rerun_iters == 0 ? (method == 5 || method == 7 ? 16 : 0)
+                                       : (o.rerun_iters < 0 ? 0 : o.rerun_iters);
     p.rerun_margin = o.rerun_margin > 0 ? o.rerun_margin : 1e-4f;
     p.rerun_pivot = o.rerun_pivot > 0 ? o.rerun_pivot : 1e-4f;
     p.init_params = o.d_init_params;
