@@ -408,6 +408,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-next-rows", action="store_true")
     ap.add_argument("--serial-parts", action="store_true", help="the method calls of a step one after the other")
+    ap.add_argument("--autotune", type=int, default=1, help="1: tune the launch shapes before timing")
+    ap.add_argument("--tune-sample", type=int, default=1_000_000, help="candidates per method the tuner times")
     ap.add_argument("--rerun-iters", type=int, default=0,
                     help="plain arm: FP64 re-run of fits with at least this many FP32 iterations (0: library "
                          "default, < 0: off)")
@@ -453,6 +455,18 @@ def main():
             nets[p.method], train_rep[p.method] = net, rep
             log(f"[bench] proposal for method {p.method} trained in {rep['wall_s']:.1f}s ({rep['labelled']} windows, "
                 f"holdout position median {rep['holdout_pos_median_px']:.3f} px)")
+    # launch shapes picked by the library's tuner on a sample of each method's
+    # candidates (kept in that method's context; fields left at 0 use them)
+    tuned = {}
+    if args.autotune and args.precision == 0:
+        for p in parts:
+            k = min(p.n, args.tune_sample)
+            t0 = time.time()
+            tuned[p.method] = p.eng.autotune(frames_dev.data_ptr(), n_frames, size, size, p.d_cands.data_ptr(), k,
+                                             p.method, w.w0, options=L.default_options(max_half_width=mh))
+            tuned[p.method]["sample"] = k
+            tuned[p.method]["wall_s"] = time.time() - t0
+            log(f"[bench] method {p.method} tuned in {time.time() - t0:.1f}s: {tuned[p.method]}")
     arm_opts = {"plain": lambda m: L.default_options(max_half_width=mh, precision=args.precision,
                                                      rerun_iters=args.rerun_iters)}
     if not args.no_warm:
@@ -575,6 +589,12 @@ def main():
             chunks.append((b0, b1, lo, hi, m, pc, po, pf))
         assert np.all(np.diff(fr_all) >= 0)
         e_eng = parts[0].eng
+        if args.autotune and args.precision == 0:
+            # the host-buffer calls run on one context: give it every method's tuned shape
+            for p in parts[1:]:
+                k = min(p.n, args.tune_sample)
+                e_eng.autotune(frames_dev.data_ptr(), n_frames, size, size, p.d_cands.data_ptr(), k, p.method, w.w0,
+                               options=L.default_options(max_half_width=mh))
         e_opts = {p.method: L.default_options(max_half_width=mh, precision=args.precision) for p in parts}
         fb = frames_pinned.element_size() * size * size
 
@@ -683,6 +703,7 @@ def main():
                 "config": {"workload": CONFIGS[args.config]["label"], "config": args.config,
                            "frames_per_gpu": n_frames, "candidates_per_gpu": n,
                            "methods": {str(p.method): p.n for p in parts}, "parallelism": f"dp{world}",
+                           "launch_shapes": {str(m): t for m, t in tuned.items()} or "library defaults",
                            "l2": f"inputs larger than L2 ({frames_dev.numel() * 2 / 1e9:.2f} GB frames)"},
                 "value_arm": "plain", "plain_lm_fits_per_s": value,
                 "plain": {"per_method": per_method, "solver_ms": k_ms},
