@@ -192,6 +192,14 @@ typedef struct loc_options {
                                   FP32 rounding moves their end point); 0: default,
                                   16 for the ellipsoidal methods 5 and 7, off for
                                   methods 0 and 1; < 0: off */
+    float rerun_skip_rejected; /* > 0: a flagged fit whose FP32 end point is
+                                  rejected by a clear margin (centre more than
+                                  this many px outside its ROI, amplitude below
+                                  zero by more than this fraction of its
+                                  offset, or every width more than this fraction
+                                  outside [0.4, 1.5] w0) is not re-run in FP64;
+                                  only its reject code could change; 0 (default):
+                                  off */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */

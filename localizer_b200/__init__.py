@@ -56,7 +56,7 @@ class Options(C.Structure):
                 ("proposal", C.c_void_p), ("warm_iter_limit", C.c_int32), ("long_rerun_iters", C.c_int32),
                 ("long_rerun_threads_per_fit", C.c_int32), ("compensated", C.c_int32),
                 ("rerun_capped", C.c_int32), ("rerun_cond", C.c_float),
-                ("rerun_iters", C.c_int32)]
+                ("rerun_iters", C.c_int32), ("rerun_skip_rejected", C.c_float)]
 
 
 class Stats(C.Structure):

@@ -174,9 +174,10 @@ template <int P>
 __global__ void k3_flag_class(const float *state32, int stride, const int *order, const int *meta,
                               const uint8_t *flags, int r, float margin, float pivot, int warm_limit, int *cls2,
                               int *order2, int *meta2, int long_iters, int *order3, int *meta3, int capped,
-                              float cond, int iters_min)
+                              float cond, int iters_min, float skip_rej, float w0)
 {
     using SL = StateLayout<P>;
+    constexpr int IX = P == 5 ? 2 : P == 4 ? 1 : 3;
     const int start = meta[m_start(r)], count = meta[m_count(r)];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         meta2[m_start(r)] = start;
@@ -200,7 +201,31 @@ __global__ void k3_flag_class(const float *state32, int stride, const int *order
                                      : (s[SL::MARGIN] < mthr || s[SL::MINPIV] < pivot || status != 0.0f ||
                                         (warm_limit > 0 && s[SL::ITERS] > (float)warm_limit) ||
                                         (iters_min > 0 && s[SL::ITERS] >= (float)iters_min));
-        if (risky) {
+        // skip_rej > 0: a fit whose FP32 end point lies clearly inside a reject
+        // rule of the finaliser (centre more than skip_rej px outside the ROI,
+        // amplitude below zero by more than skip_rej of its start scale, or
+        // every width more than the fraction skip_rej outside its accepted
+        // range) is not re-run: only its reject code could change
+        bool clear_reject = false;
+        if (risky && skip_rej > 0.0f) {
+            const float side = (float)(2 * r);
+            const float x = s[IX], y = s[IX + 1], A = s[0];
+            clear_reject = x < -skip_rej || x > side + skip_rej || y < -skip_rej || y > side + skip_rej ||
+                           A < -skip_rej * fmaxf(fabsf(s[P - 1]), 1.0f);
+            const float lo = 0.4f * w0 * (1.0f - skip_rej), hi = 1.5f * w0 * (1.0f + skip_rej);
+            if constexpr (P == 5) {
+                const float wd = fabsf(s[1]);
+                clear_reject = clear_reject || wd < lo || wd > hi;
+            } else if constexpr (P == 7) {
+                // axes of the covariance [[sx^2, rho sx sy], [rho sx sy, sy^2]]
+                const float sx = fabsf(s[1]), sy = fabsf(s[2]), rho = s[5];
+                const float a = sx * sx, c = sy * sy, b = rho * sx * sy;
+                const float ht = 0.5f * (a + c), rad = sqrtf(0.25f * (a - c) * (a - c) + b * b);
+                const float s1 = sqrtf(fmaxf(ht - rad, 0.0f)), s2 = sqrtf(ht + rad);
+                clear_reject = clear_reject || ((s1 < lo || s1 > hi) && (s2 < lo || s2 > hi));
+            }
+        }
+        if (risky && !clear_reject) {
             cls2[i] = r;
             if (meta3 && s[SL::ITERS] > (float)long_iters) {
                 const int slot = atomicAdd(&meta3[m_count(r)], 1);
@@ -1359,13 +1384,13 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
                 switch (m) {
                 case 0: k3_flag_class<5><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r, p.rerun_margin,
                                                              p.rerun_pivot, wl, s.cls2, s.order2, s.meta2, li, o3,
-                                                             m3, p.rerun_capped, p.rerun_cond, p.rerun_iters); break;
+                                                             m3, p.rerun_capped, p.rerun_cond, p.rerun_iters, p.rerun_skip_rejected, (float)p.w0); break;
                 case 1: k3_flag_class<4><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r, p.rerun_margin,
                                                              p.rerun_pivot, wl, s.cls2, s.order2, s.meta2, li, o3,
-                                                             m3, p.rerun_capped, p.rerun_cond, p.rerun_iters); break;
+                                                             m3, p.rerun_capped, p.rerun_cond, p.rerun_iters, p.rerun_skip_rejected, (float)p.w0); break;
                 default: k3_flag_class<7><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r,
                                                               p.rerun_margin, p.rerun_pivot, wl, s.cls2, s.order2,
-                                                              s.meta2, li, o3, m3, p.rerun_capped, p.rerun_cond, p.rerun_iters); break;
+                                                              s.meta2, li, o3, m3, p.rerun_capped, p.rerun_cond, p.rerun_iters, p.rerun_skip_rejected, (float)p.w0); break;
                 }
                 if ((e = cudaGetLastError()) != cudaSuccess) return e;
                 bump();

@@ -58,6 +58,7 @@ struct FitParams {
     int rerun_capped;          // also re-run in FP64 the fits FP32 stopped at the iteration cap
     float rerun_cond;          // > 0: margin threshold raised to rerun_cond * eps32 / smallest pivot ratio
     int rerun_iters;           // > 0: also re-run fits whose FP32 solve took at least this many iterations
+    float rerun_skip_rejected; // > 0: flagged fits that end clearly rejected in FP32 are not re-run
     float rerun_margin;        // branch-decision margin below which a fit is flagged
     float rerun_pivot;         // undamped pivot ratio below which a fit is flagged
     const float *init_params;
