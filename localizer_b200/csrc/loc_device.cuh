@@ -236,8 +236,7 @@ __device__ __forceinline__ void pass_sym(const float *__restrict__ roi, int ld, 
             const T wy = (T)j - y0;
             body(i, wy, wy * wy, -dxs * dxs - dys * (T(2) * wy + dys), roi + j * s * ld);
         }
-        return;
-    }
+    } else {
 #pragma unroll 1
     for (int j = 0; j < s; ++j) {
         const T wy = (T)j - y0;
@@ -256,6 +255,7 @@ __device__ __forceinline__ void pass_sym(const float *__restrict__ roi, int ld, 
 #pragma unroll 1
             for (int i = q; i < s; i += TPF) body(i, wy, wy2, krow, row);
         }
+    }
     }
 }
 
@@ -305,8 +305,7 @@ __device__ __forceinline__ void pass_fixed(const float *__restrict__ roi, int ld
             const T wy = (T)j - y0;
             body(i, wy, wy * wy, -dxs * dxs - dys * (T(2) * wy + dys), roi + j * s * ld);
         }
-        return;
-    }
+    } else {
 #pragma unroll 1
     for (int j = 0; j < s; ++j) {
         const T wy = (T)j - y0;
@@ -325,6 +324,7 @@ __device__ __forceinline__ void pass_fixed(const float *__restrict__ roi, int ld
 #pragma unroll 1
             for (int i = q; i < s; i += TPF) body(i, wy, wy2, krow, row);
         }
+    }
     }
 }
 
@@ -418,8 +418,7 @@ __device__ __forceinline__ void pass_ell(const float *__restrict__ roi, int ld, 
             row_terms(j, wy, wy2, wc, wrb, brow, crow);
             body(i, wy, wy2, wc, wrb, brow, crow, roi + j * s * ld);
         }
-        return;
-    }
+    } else {
 #pragma unroll 1
     for (int j = 0; j < s; ++j) {
         const T wy = (T)j - y0;
@@ -444,6 +443,7 @@ __device__ __forceinline__ void pass_ell(const float *__restrict__ roi, int ld, 
 #pragma unroll 1
             for (int i = q; i < s; i += TPF) body(i, wy, wy2, wc, wrb, brow, crow, row);
         }
+    }
     }
 }
 
