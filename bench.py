@@ -71,6 +71,10 @@ XCOL = {0: 3, 1: 2, 5: 4, 7: 4}
 # exists
 TRAFFIC_PER_FIT = {"bytes": 1925.0, "source": "profiles/launches_dense500_plain.md (dense workload, 500 frames)"}
 
+# the launch-shape fields of loc_options that the tuner picks
+SHAPE_KEYS = ("threads_per_fit", "tail_threads_per_fit", "level0_budget", "rerun_threads_per_fit",
+              "long_rerun_threads_per_fit", "threads_per_block")
+
 CONFIGS = {
     1: {"workload": "small", "block": 0,
         "label": "plain method, small: 512 frames 128x128 uint16, 50 emitters/frame, symmetric PSF sigma 1.3, "
@@ -81,6 +85,11 @@ CONFIGS = {
     3: {"workload": "stress", "block": 0,
         "label": "precision stress: 5000 frames 256x256 uint16, 50 emitters/frame, amplitude U[50,200], "
                  "background 150, 10% of emitters 1.5-3 px from a neighbour, sigma 1.5, 11x11 ROI, method 0"},
+    4: {"workload": "uneven", "block": 0, "train_rois": 2_000_000,
+        "label": "learned proposal: network trained on 2M synthetic 11x11 forward-model windows (sigma U[1,2], "
+                 "amplitude lognormal median 500, background U[50,200], Poisson + read noise, offsets U[-1,1] px) "
+                 "labelled by the plain LM fit, applied as the warm start to the batched uneven workload "
+                 "(10000 frames 256x256, method 7)"},
     5: {"workload": "dense", "block": 5000,
         "label": "large dense: 50000 frames 512x512 uint16 (26.2 GB resident), 300-1000 emitters/frame, "
                  "sigma U[1,2], ROI 7/9/11/13, symmetric (method 0) and ellipsoidal (method 7) fits in "
@@ -449,8 +458,10 @@ def main():
     if not args.no_warm:
         for p in parts:
             t_tr = time.time()
-            net, rep = PR.train(method=p.method, n_rois=0, frames=args.train_frames, epochs=args.train_epochs,
-                                seed=7 + 1000 * rank, device=local, workload=CONFIGS[args.config]["workload"])
+            n_syn = CONFIGS[args.config].get("train_rois", 0)
+            net, rep = PR.train(method=p.method, n_rois=n_syn, frames=0 if n_syn else args.train_frames,
+                                epochs=args.train_epochs, seed=7 + 1000 * rank, device=local,
+                                workload=CONFIGS[args.config]["workload"])
             rep["wall_s"] = time.time() - t_tr
             nets[p.method], train_rep[p.method] = net, rep
             log(f"[bench] proposal for method {p.method} trained in {rep['wall_s']:.1f}s ({rep['labelled']} windows, "
@@ -531,8 +542,10 @@ def main():
 
     res = {}
     for arm in opts:
-        res[arm] = timed(arm, args.steps if arm in ("plain", "warm") else max(3, args.steps // 4))
-        log(f"[bench] arm {arm}: {res[arm]['value'] / 1e6:.2f} M fits/s, {res[arm]['ms'] / args.steps:.1f} ms/step")
+        k_steps = args.steps if arm in ("plain", "warm") else max(3, args.steps // 4)
+        res[arm] = timed(arm, k_steps)
+        res[arm]["steps"] = k_steps
+        log(f"[bench] arm {arm}: {res[arm]['value'] / 1e6:.2f} M fits/s, {res[arm]['ms'] / k_steps:.1f} ms/step")
     value = res["plain"]["value"]
     elapsed_ms = res["plain"]["ms"]
 
@@ -589,13 +602,12 @@ def main():
             chunks.append((b0, b1, lo, hi, m, pc, po, pf))
         assert np.all(np.diff(fr_all) >= 0)
         e_eng = parts[0].eng
-        if args.autotune and args.precision == 0:
-            # the host-buffer calls run on one context: give it every method's tuned shape
-            for p in parts[1:]:
-                k = min(p.n, args.tune_sample)
-                e_eng.autotune(frames_dev.data_ptr(), n_frames, size, size, p.d_cands.data_ptr(), k, p.method, w.w0,
-                               options=L.default_options(max_half_width=mh))
-        e_opts = {p.method: L.default_options(max_half_width=mh, precision=args.precision) for p in parts}
+        # the host-buffer calls run on one context: each method's tuned
+        # launch shape is passed explicitly, so the rows match the device
+        # path's bit for bit
+        e_opts = {p.method: L.default_options(max_half_width=mh, precision=args.precision,
+                                              **{k: tuned[p.method][k] for k in SHAPE_KEYS if p.method in tuned})
+                  for p in parts}
         fb = frames_pinned.element_size() * size * size
 
         def e2e_step():

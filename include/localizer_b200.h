@@ -89,9 +89,10 @@ typedef struct loc_candidate {
 } loc_candidate;
 
 /* Precision of the iterative solve. FP32 is the production path (FP32
- * model, Jacobian and normal equations; FP64 only for ill-conditioned
- * Cholesky pivots and for the final covariance). FP64 runs the same
- * algorithm entirely in double precision (for accuracy studies). */
+ * model, Jacobian and normal equations; fits whose FP32 outcome could depend
+ * on FP32 rounding are re-run in FP64, see fp64_rerun and the rerun_*
+ * fields; the final covariance and columns are FP64). FP64 runs the same
+ * algorithm entirely in double precision for every fit. */
 #define LOC_PRECISION_FP32 0
 #define LOC_PRECISION_FP64 1
 
@@ -106,7 +107,8 @@ typedef struct loc_options {
                                   fits are re-run in FP64 instead (fp64_rerun) */
     int32_t threads_per_block; /* 0: tuned default */
     int32_t blocks_per_sm;     /* 0: occupancy maximum */
-    int32_t stage_u16;         /* -1: tuned; 0: ROI staged as float; 1: as uint16 */
+    int32_t stage_u16;         /* reserved, ignored: ROIs are staged in shared
+                                  memory as FP32 (kept for the struct layout) */
     int32_t max_half_width;    /* 0: the solver reads the largest ROI half-width
                                   present back from the device (one small
                                   synchronous copy); > 0: caller guarantees
@@ -198,8 +200,9 @@ typedef struct loc_options {
                                   zero by more than this fraction of its
                                   offset, or every width more than this fraction
                                   outside [0.4, 1.5] w0) is not re-run in FP64;
-                                  only its reject code could change; 0 (default):
-                                  off */
+                                  only its reject code could change; 0
+                                  (default): 0.5 for the ellipsoidal methods 5
+                                  and 7, off for methods 0 and 1; < 0: off */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */

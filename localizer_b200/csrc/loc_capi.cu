@@ -285,7 +285,8 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     // and fixed-width fits keep their FP32 end points to 1e-3 px without it)
     p.rerun_iters = o.rerun_iters == 0 ? (method == 5 || method == 7 ? 16 : 0)
                                        : (o.rerun_iters < 0 ? 0 : o.rerun_iters);
-    p.rerun_skip_rejected = o.rerun_skip_rejected > 0 ? o.rerun_skip_rejected : 0.0f;
+    p.rerun_skip_rejected = o.rerun_skip_rejected == 0.0f ? (method == 5 || method == 7 ? 0.5f : 0.0f)
+                                                          : (o.rerun_skip_rejected < 0.0f ? 0.0f : o.rerun_skip_rejected);
     p.rerun_margin = o.rerun_margin > 0 ? o.rerun_margin : 1e-4f;
     p.rerun_pivot = o.rerun_pivot > 0 ? o.rerun_pivot : 1e-4f;
     p.long_rerun_threads_per_fit = o.long_rerun_threads_per_fit > 0 ? o.long_rerun_threads_per_fit : 8;

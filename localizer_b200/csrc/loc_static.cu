@@ -156,7 +156,8 @@ extern "C" LOC_API int loc_fit_batch_static(const uint16_t *d_frames, int n_fram
     // and fixed-width fits keep their FP32 end points to 1e-3 px without it)
     p.rerun_iters = o.rerun_iters == 0 ? (method == 5 || method == 7 ? 16 : 0)
                                        : (o.rerun_iters < 0 ? 0 : o.rerun_iters);
-    p.rerun_skip_rejected = o.rerun_skip_rejected > 0 ? o.rerun_skip_rejected : 0.0f;
+    p.rerun_skip_rejected = o.rerun_skip_rejected == 0.0f ? (method == 5 || method == 7 ? 0.5f : 0.0f)
+                                                          : (o.rerun_skip_rejected < 0.0f ? 0.0f : o.rerun_skip_rejected);
     p.rerun_margin = o.rerun_margin > 0 ? o.rerun_margin : 1e-4f;
     p.rerun_pivot = o.rerun_pivot > 0 ? o.rerun_pivot : 1e-4f;
     p.init_params = o.d_init_params;

@@ -331,6 +331,7 @@ def train(method: int = 7, n_rois: int = 2_000_000, epochs: int = 8, batch: int 
     ix, iy = roles.index(2), roles.index(3)
     rep = {"method": method, "windows": n_rois, "labelled": int(valid.sum().item()), "epochs": epochs,
            "batch": batch, "steps": step, "data_s": t_data, "train_s": t_train,
+           "train_windows_per_s": step * batch / max(t_train, 1e-9),
            "loss_initial": loss0, "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1],
            "loss_probe": f"weighted squared error on {len(probe)} held-out windows after each epoch",
            "loss_weights": lam.tolist(),
