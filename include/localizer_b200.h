@@ -202,7 +202,10 @@ typedef struct loc_options {
                                   outside [0.4, 1.5] w0) is not re-run in FP64;
                                   only its reject code could change; 0
                                   (default): 0.5 for the ellipsoidal methods 5
-                                  and 7, off for methods 0 and 1; < 0: off */
+                                  and 7, off for methods 0 and 1; < 0: off;
+                                  never applied with a proposal (a warm fit's
+                                  end point says nothing about the reference
+                                  start's) */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */

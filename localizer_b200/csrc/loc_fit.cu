@@ -1381,16 +1381,19 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
                 const int sst = state_stride(p.method);
                 int *o3 = long_q ? s.order3 : nullptr, *m3 = long_q ? s.meta3 : nullptr;
                 const int li = p.long_rerun_iters;
+                // a warm fit's reject says nothing about where the reference
+                // start's path ends: with a proposal every flagged fit is re-run
+                const float skip = p.warm ? 0.0f : p.rerun_skip_rejected;
                 switch (m) {
                 case 0: k3_flag_class<5><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r, p.rerun_margin,
                                                              p.rerun_pivot, wl, s.cls2, s.order2, s.meta2, li, o3,
-                                                             m3, p.rerun_capped, p.rerun_cond, p.rerun_iters, p.rerun_skip_rejected, (float)p.w0); break;
+                                                             m3, p.rerun_capped, p.rerun_cond, p.rerun_iters, skip, (float)p.w0); break;
                 case 1: k3_flag_class<4><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r, p.rerun_margin,
                                                              p.rerun_pivot, wl, s.cls2, s.order2, s.meta2, li, o3,
-                                                             m3, p.rerun_capped, p.rerun_cond, p.rerun_iters, p.rerun_skip_rejected, (float)p.w0); break;
+                                                             m3, p.rerun_capped, p.rerun_cond, p.rerun_iters, skip, (float)p.w0); break;
                 default: k3_flag_class<7><<<fb, 256, 0, cs>>>(st32, sst, s.order, s.meta, p.flags, r,
                                                               p.rerun_margin, p.rerun_pivot, wl, s.cls2, s.order2,
-                                                              s.meta2, li, o3, m3, p.rerun_capped, p.rerun_cond, p.rerun_iters, p.rerun_skip_rejected, (float)p.w0); break;
+                                                              s.meta2, li, o3, m3, p.rerun_capped, p.rerun_cond, p.rerun_iters, skip, (float)p.w0); break;
                 }
                 if ((e = cudaGetLastError()) != cudaSuccess) return e;
                 bump();
