@@ -71,6 +71,9 @@ XCOL = {0: 3, 1: 2, 5: 4, 7: 4}
 # exists
 TRAFFIC_PER_FIT = {"bytes": 1925.0, "source": "profiles/launches_dense500_plain.md (dense workload, 500 frames)"}
 
+# the two reference builds: strict FP64 (the yardstick) and the reference's
+# own release flags (LinuxCompile.sh), which time the CPU baseline
+REF_BUILD = {False: "-O2, no fast-math", True: "-O2 -ffast-math, the reference's release flags"}
 # the launch-shape fields of loc_options that the tuner picks
 SHAPE_KEYS = ("threads_per_fit", "tail_threads_per_fit", "level0_budget", "rerun_threads_per_fit",
               "long_rerun_threads_per_fit", "threads_per_block")
@@ -216,11 +219,12 @@ def make_workload(w):
     return frames_dev, cands, finder
 
 
-def ref_fit_parallel(frames_host, cands, methods, w0, threads):
-    """The reference's own fitter (oracle/_ref) over the candidates, whole
-    frames per host thread, one fitter call per (frame, half-width, method)
-    group as the reference's workers make them. Returns (seconds, rows per
-    method {m: (idx, rows, kept, iters)})."""
+def ref_fit_parallel(frames_host, cands, methods, w0, threads, fast=False):
+    """The reference's own fitter (oracle/_ref; fast=True: its release-flag
+    build) over the candidates, whole frames per host thread, one fitter call
+    per (frame, half-width, method) group as the reference's workers make
+    them. Returns (seconds, rows per method {m: (idx, rows, kept, iters)},
+    threads)."""
     from oracle import oracle as O
     frame_ids = np.unique(cands["frame"])
     chunks = [c for c in np.array_split(frame_ids, threads) if len(c)]
@@ -231,7 +235,7 @@ def ref_fit_parallel(frames_host, cands, methods, w0, threads):
         part = {}
         for m in np.unique(methods[m_sel]):
             idx = np.nonzero(m_sel & (methods == m))[0]
-            out, kp, it, _ = O.ref_fit(frames_host, np.ascontiguousarray(cands[idx]), int(m), w0)
+            out, kp, it, _ = O.ref_fit(frames_host, np.ascontiguousarray(cands[idx]), int(m), w0, fast=fast)
             part[int(m)] = (idx, out, kp == 1, it)
         results[k] = part
 
@@ -356,14 +360,15 @@ def reference_arm(args):
         f"{time.time() - t0:.1f}s; {budget:.1f}s of fits per step on {threads} threads")
     vals = []
     th = threads
+    fast = O.ref_fast_available()
     for step in range(args.warmup + args.steps):
-        dt, _, th = ref_fit_parallel(frames, cands, methods, w.w0, threads)
+        dt, _, th = ref_fit_parallel(frames, cands, methods, w.w0, threads, fast=fast)
         if step >= args.warmup:
             vals.append(len(cands) / dt)
     value = float(np.mean(vals))
     sample = (f"{len(cands)} candidates of {len(chosen)} whole frames spread through the stack per step "
-              f"(host-rendered from the configuration's seeded emitters); reference Localization.cpp FP64 + "
-              f"lmsder restatement, {th} threads")
+              f"(host-rendered from the configuration's seeded emitters); reference Localization.cpp FP64 "
+              f"({REF_BUILD[fast]}) + lmsder restatement, {th} threads")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * len(cands) / value, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded emitters; host-rendered frames)",
@@ -667,7 +672,16 @@ def main():
             dt, ref, th = ref_fit_parallel(frames_host, cands[sel], methods[sel], w.w0, threads)
             cpu = {"value": len(sel) / dt, "unit": UNIT, "cores": th, "kind": "reference",
                    "sample": f"{len(sel)} candidates of {len(chosen)} whole frames spread through the stack; "
-                             f"reference Localization.cpp FP64 + lmsder restatement, {th} host threads"}
+                             f"reference Localization.cpp FP64 ({REF_BUILD[False]}) + lmsder restatement, "
+                             f"{th} host threads"}
+            if O.ref_fast_available():
+                # the same sample through the reference's release build: the
+                # baseline's value (the strict build above gives the accuracy)
+                dt_f, _, _ = ref_fit_parallel(frames_host, cands[sel], methods[sel], w.w0, threads, fast=True)
+                cpu["strict_fits_per_s"] = cpu["value"]
+                cpu["value"] = len(sel) / dt_f
+                cpu["sample"] = cpu["sample"].replace(REF_BUILD[False], REF_BUILD[True] + "; the strict build's rate "
+                                                      "is strict_fits_per_s")
             accuracy = {"sample_fits": int(len(sel)), "reference": "reference fitter (FP64) on the same candidates",
                         "classes": "converged fits beyond 1e-3 px: rounding_sensitive (the GPU's all-FP64 solve "
                                    "misses too) or fp32_only"}

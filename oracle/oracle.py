@@ -19,6 +19,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libloc_ref.so")
+REF_FAST_SO = os.path.join(HERE, "_ref", "libloc_ref_fast.so")
 CAPI_SO = os.path.join(HERE, "_ref", "libfitpositions_gpu.so")
 
 CAND_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("intensity", "<f8"), ("background", "<f8"),
@@ -36,6 +37,7 @@ class _Options(C.Structure):
 
 _lib = None
 _ref = None
+_ref_fast = None
 
 
 # the reference tree the Makefile compiles from: $LOC_REFERENCE, else the
@@ -54,7 +56,7 @@ def build():
     ref = reference_tree()
     targets = ["oracle"]
     if os.path.isdir(os.path.join(ref, "source")):
-        targets += ["ref", "capi"]
+        targets += ["ref", "reffast", "capi"]
     subprocess.run(["make", "-s", "-C", HERE, f"REF={ref}"] + targets, check=True)
 
 
@@ -88,25 +90,39 @@ def ref_available() -> bool:
     return os.path.exists(REF_SO)
 
 
-def ref():
-    global _ref
+def ref_fast_available() -> bool:
+    return os.path.exists(REF_FAST_SO)
+
+
+def ref(fast: bool = False):
+    """The reference build (strict FP64: the yardstick), or with fast=True
+    the same sources built with the reference's release flags (-O2
+    -ffast-math), for timing only."""
+    global _ref, _ref_fast
+    if fast:
+        if _ref_fast is None:
+            _ref_fast = _bind_ref(C.CDLL(REF_FAST_SO))
+        return _ref_fast
     if _ref is None:
-        L = C.CDLL(REF_SO)
-        L.ref_fit.restype = C.c_int
-        L.ref_fit.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
-                              C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
-        L.ref_find_adjacent8.restype = C.c_int
-        L.ref_find_adjacent8.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
-        L.ref_glrt_mask.restype = C.c_int
-        L.ref_glrt_mask.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p]
-        L.ref_find_candidates.restype = C.c_long
-        L.ref_find_candidates.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
-                                          C.c_void_p, C.c_long]
-        L.ref_write_positions.restype = C.c_int
-        L.ref_write_positions.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
-                                          C.c_double, C.c_double, C.c_char_p, C.c_char_p]
-        _ref = L
+        _ref = _bind_ref(C.CDLL(REF_SO))
     return _ref
+
+
+def _bind_ref(L):
+    L.ref_fit.restype = C.c_int
+    L.ref_fit.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                          C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.ref_find_adjacent8.restype = C.c_int
+    L.ref_find_adjacent8.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+    L.ref_glrt_mask.restype = C.c_int
+    L.ref_glrt_mask.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p]
+    L.ref_find_candidates.restype = C.c_long
+    L.ref_find_candidates.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                      C.c_void_p, C.c_long]
+    L.ref_write_positions.restype = C.c_int
+    L.ref_write_positions.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                      C.c_double, C.c_double, C.c_char_p, C.c_char_p]
+    return L
 
 
 def _stack_dims(frames: np.ndarray):
@@ -274,9 +290,10 @@ def group_for_reference(cands):
     return np.lexsort((cands["half_width"], cands["frame"]))
 
 
-def ref_fit(frames, cands, method, w0, sigma=1.0):
-    """The reference's own fitter classes. Returns (out[nc, cols], kept[nc],
-    iters[nc], status[nc]) in the order of ``cands`` (grouped internally)."""
+def ref_fit(frames, cands, method, w0, sigma=1.0, fast=False):
+    """The reference's own fitter classes (fast=True: the release-flag build).
+    Returns (out[nc, cols], kept[nc], iters[nc], status[nc]) in the order of
+    ``cands`` (grouped internally)."""
     n_frames, n_rows, n_cols = _stack_dims(frames)
     cands = np.ascontiguousarray(cands, dtype=CAND_DTYPE)
     order = group_for_reference(cands)
@@ -287,7 +304,7 @@ def ref_fit(frames, cands, method, w0, sigma=1.0):
     kept = np.zeros(nc, dtype=np.int32)
     iters = np.zeros(nc, dtype=np.int32)
     status = np.zeros(nc, dtype=np.int32)
-    rc = ref().ref_fit(frames.ctypes.data, n_frames, n_rows, n_cols, cs.ctypes.data, nc, method, w0,
+    rc = ref(fast).ref_fit(frames.ctypes.data, n_frames, n_rows, n_cols, cs.ctypes.data, nc, method, w0,
                        sigma, out.ctypes.data, kept.ctypes.data, iters.ctypes.data, status.ctypes.data)
     if rc != 0:
         raise ValueError(f"ref_fit failed: {rc}")
