@@ -423,7 +423,8 @@ def main():
     ap.add_argument("--no-next-rows", action="store_true")
     ap.add_argument("--serial-parts", action="store_true", help="the method calls of a step one after the other")
     ap.add_argument("--autotune", type=int, default=1, help="1: tune the launch shapes before timing")
-    ap.add_argument("--tune-sample", type=int, default=1_000_000, help="candidates per method the tuner times")
+    ap.add_argument("--tune-sample", type=int, default=0,
+                    help="candidates per method the tuner times (0: all of the method's candidates)")
     ap.add_argument("--rerun-iters", type=int, default=0,
                     help="plain arm: FP64 re-run of fits with at least this many FP32 iterations (0: library "
                          "default, < 0: off)")
@@ -476,7 +477,7 @@ def main():
     tuned = {}
     if args.autotune and args.precision == 0:
         for p in parts:
-            k = min(p.n, args.tune_sample)
+            k = min(p.n, args.tune_sample) if args.tune_sample > 0 else p.n
             t0 = time.time()
             tuned[p.method] = p.eng.autotune(frames_dev.data_ptr(), n_frames, size, size, p.d_cands.data_ptr(), k,
                                              p.method, w.w0, options=L.default_options(max_half_width=mh))
@@ -635,17 +636,23 @@ def main():
             torch.distributed.barrier()
         dstream = torch.cuda.default_stream()
         s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        hb0 = e_eng.host_bytes()
         s2.record(dstream)
         for _ in range(e_steps):
             e2e_step()
         wait()
         e2.record(dstream)
         torch.cuda.synchronize()
+        hb1 = e_eng.host_bytes()
         _, e_ms, e_rate = DI.job_throughput(n * e_steps, s2.elapsed_time(e2))
-        e2e = {"value": e_rate, "unit": UNIT, "h2d_bytes_per_step": int(frames_dev.numel() * 2 + cands.nbytes),
-               "d2h_bytes_per_step": int(sum(po.numel() * 8 + pf.numel() for *_, po, pf in chunks)), "arm": "plain",
+        # bytes the library copied (its own count: with the ROI upload only the
+        # candidates' ROIs cross PCIe, gathered on the host inside the calls)
+        e2e = {"value": e_rate, "unit": UNIT, "h2d_bytes_per_step": int((hb1[0] - hb0[0]) // e_steps),
+               "d2h_bytes_per_step": int((hb1[1] - hb0[1]) // e_steps), "arm": "plain",
+               "frame_bytes_per_step": int(frames_dev.numel() * 2),
                "call": f"loc_fit_host_async per block of {blk} frames ({len(chunks)} calls per step, pinned host "
-                       f"buffers, uploads overlapping the previous call's fit), loc_fit_host_wait at the end",
+                       f"buffers, uploads overlapping the previous call's fit, ROI upload where the "
+                       f"candidates' ROIs are under 3/4 of the frames), loc_fit_host_wait at the end",
                "steps": e_steps, "ms_per_step": e_ms / e_steps}
         # the host-buffer path gives the device path's rows
         for b0, b1, lo, hi, m, pc, po, pf in chunks:

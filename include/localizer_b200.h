@@ -206,6 +206,13 @@ typedef struct loc_options {
                                   never applied with a proposal (a warm fit's
                                   end point says nothing about the reference
                                   start's) */
+    int32_t host_roi_mode;     /* loc_fit_host / loc_fit_host_async: 0
+                                  (default): when the candidates' ROIs hold
+                                  fewer than 3/4 of the stack's pixels, only
+                                  they cross PCIe (gathered on the host into
+                                  one slot per candidate; rows identical to
+                                  the whole-frame upload); not with a proposal
+                                  or method 6; < 0: always upload whole frames */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */
@@ -255,7 +262,10 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
                           uint8_t *d_flags, void *stream);
 
 /* Same fit with host buffers: copies frames and candidates to the device,
- * fits and copies rows and flags back (the whole path a host caller sees). */
+ * fits and copies rows and flags back (the whole path a host caller sees).
+ * Where the candidates' ROIs are a small part of the frames (host_roi_mode),
+ * the host threads gather each candidate's ROI into a slot and only the
+ * slots are copied; the solver reads the same pixels from them. */
 LOC_API int loc_fit_host(loc_ctx *ctx, const uint16_t *frames, int n_frames, int n_rows,
                          int n_cols, const loc_candidate *cands, int n_cands, int method,
                          double w0, double sigma, const loc_options *opt, double *out,
@@ -280,6 +290,10 @@ LOC_API int loc_fit_host_async(loc_ctx *ctx, const uint16_t *frames, int n_frame
 /* Waits for every loc_fit_host_async call of the context; reports the first
  * device error of those calls. */
 LOC_API int loc_fit_host_wait(loc_ctx *ctx);
+
+/* Bytes the context's host-buffer calls (loc_fit_host, loc_fit_host_async)
+ * have copied host -> device and device -> host since it was created. */
+LOC_API int loc_host_bytes(const loc_ctx *ctx, uint64_t *h2d, uint64_t *d2h);
 
 /*
  * Allocation-free form of loc_fit_batch (same arguments, no context, same

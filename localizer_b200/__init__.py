@@ -56,7 +56,8 @@ class Options(C.Structure):
                 ("proposal", C.c_void_p), ("warm_iter_limit", C.c_int32), ("long_rerun_iters", C.c_int32),
                 ("long_rerun_threads_per_fit", C.c_int32), ("compensated", C.c_int32),
                 ("rerun_capped", C.c_int32), ("rerun_cond", C.c_float),
-                ("rerun_iters", C.c_int32), ("rerun_skip_rejected", C.c_float)]
+                ("rerun_iters", C.c_int32), ("rerun_skip_rejected", C.c_float),
+                ("host_roi_mode", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -100,6 +101,7 @@ _PROTOS = {
     "loc_fit_host_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                      C.c_int, C.c_double, C.c_double, C.POINTER(Options), C.c_void_p, C.c_void_p]),
     "loc_fit_host_wait": (C.c_int, [C.c_void_p]),
+    "loc_host_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "loc_fit_batch_static": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                        C.c_double, C.c_double, C.POINTER(Options), C.c_void_p, C.c_void_p,
                                        C.c_void_p]),
@@ -285,6 +287,13 @@ class Engine:
             _check(lib().loc_fit_host_wait(self._h))
         finally:
             self._inflight = []
+
+    def host_bytes(self):
+        """loc_host_bytes: (host -> device, device -> host) bytes copied by
+        the context's host-buffer calls so far."""
+        h2d, d2h = C.c_uint64(), C.c_uint64()
+        _check(lib().loc_host_bytes(self._h, C.byref(h2d), C.byref(d2h)))
+        return h2d.value, d2h.value
 
 
 _default_engine = None

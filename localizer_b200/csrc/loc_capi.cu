@@ -11,6 +11,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -58,13 +59,146 @@ struct DevBuf {
     }
 };
 
+// Page-locked host buffer, grown on demand (the ROI staging of host calls).
+struct HostBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes)
+    {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = bytes + bytes / 8 + 4096;
+        cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    void release()
+    {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+// ROI mode of the host-buffer calls. Instead of whole frames, each candidate
+// that the fit's input and edge rules keep (the rules of k0_classify, the
+// reference's Localization.cpp:115-124) gets a slot of side x side pixels
+// holding its (2r+1)^2 ROI at the slot's origin, side = 2 rmax + 1 over the
+// call; only the slots cross PCIe. The solver reads the same pixels from the
+// slots, so the rows are those of the frame upload.
+struct RoiPlan {
+    bool use = false;
+    int slots = 0, side = 0;
+};
+
+int host_threads()
+{
+    const unsigned hc = std::thread::hardware_concurrency();
+    return (int)std::max(1u, std::min(hc ? hc : 1u, 32u));
+}
+
+// slot_of[i]: the candidate's slot, -1 for a candidate the fit rejects before
+// reading pixels. Gathers into roi (slots x side^2 uint16) when the slots
+// hold fewer bytes than max_fraction of the frames.
+RoiPlan plan_and_gather_rois(const uint16_t *frames, int n_frames, int n_rows, int n_cols, const loc_candidate *c,
+                             int n, double w0, int max_half_width, double max_fraction, int *slot_of,
+                             HostBuf *roi, cudaError_t *err)
+{
+    RoiPlan plan;
+    *err = cudaSuccess;
+    if (n <= 0) return plan;
+    const int r_default = (int)std::ceil(w0 * 4.0);
+    const int r_cap = max_half_width > 0 ? std::min(max_half_width, locb::kMaxHalfWidth) : locb::kMaxHalfWidth;
+    const int nt = std::min(host_threads(), std::max(1, n / 4096));
+    std::vector<int> cnt(nt, 0), rmax(nt, 0);
+    auto chunk = [&](int t, int &lo, int &hi) {
+        lo = (int)((long long)n * t / nt);
+        hi = (int)((long long)n * (t + 1) / nt);
+    };
+    auto run = [&](auto fn) {
+        std::vector<std::thread> th;
+        for (int t = 1; t < nt; ++t) th.emplace_back(fn, t);
+        fn(0);
+        for (auto &x : th) x.join();
+    };
+    // pass 1: which candidates read pixels, and the largest ROI
+    run([&](int t) {
+        int lo, hi, k = 0, rm = 0;
+        chunk(t, lo, hi);
+        for (int i = lo; i < hi; ++i) {
+            const loc_candidate &q = c[i];
+            const bool finite = std::isfinite(q.x) && std::isfinite(q.y) && std::isfinite(q.intensity) &&
+                                std::isfinite(q.background);
+            const int r = q.half_width > 0 ? q.half_width : r_default;
+            int slot = -1;
+            if (finite && q.frame >= 0 && q.frame < n_frames && q.half_width >= 0 && r >= 1 && r <= r_cap) {
+                const double xo = std::floor(q.x - (double)r), yo = std::floor(q.y - (double)r);
+                if (!(xo < 0 || xo + 2 * r > n_rows - 1 || yo < 0 || yo + 2 * r > n_cols - 1)) {
+                    slot = k++;
+                    rm = std::max(rm, r);
+                }
+            }
+            slot_of[i] = slot;
+        }
+        cnt[t] = k;
+        rmax[t] = rm;
+    });
+    std::vector<int> base(nt, 0);
+    int total = 0, rm = 0;
+    for (int t = 0; t < nt; ++t) {
+        base[t] = total;
+        total += cnt[t];
+        rm = std::max(rm, rmax[t]);
+    }
+    if (total == 0) return plan;
+    const int side = 2 * rm + 1;
+    const double roi_bytes = (double)total * side * side * sizeof(uint16_t);
+    const double frame_bytes = (double)n_frames * n_rows * n_cols * sizeof(uint16_t);
+    if (!(roi_bytes < max_fraction * frame_bytes)) return plan;
+    if ((*err = roi->ensure((size_t)roi_bytes)) != cudaSuccess) return plan;
+    uint16_t *dst0 = (uint16_t *)roi->p;
+    const size_t fpx = (size_t)n_rows * n_cols;
+    // pass 2: slot numbers in candidate order, rows copied into the slots
+    run([&](int t) {
+        int lo, hi;
+        chunk(t, lo, hi);
+        for (int i = lo; i < hi; ++i) {
+            if (slot_of[i] < 0) continue;
+            const int slot = (slot_of[i] += base[t]);
+            const loc_candidate &q = c[i];
+            const int r = q.half_width > 0 ? q.half_width : r_default;
+            const int sd = 2 * r + 1;
+            const size_t xo = (size_t)std::floor(q.x - (double)r), yo = (size_t)std::floor(q.y - (double)r);
+            const uint16_t *src = frames + (size_t)q.frame * fpx + xo + yo * (size_t)n_rows;
+            uint16_t *dst = dst0 + (size_t)slot * side * side;
+            for (int j = 0; j < sd; ++j)
+                std::memcpy(dst + (size_t)j * side, src + (size_t)j * n_rows, (size_t)sd * sizeof(uint16_t));
+        }
+    });
+    plan.use = true;
+    plan.slots = total;
+    plan.side = side;
+    return plan;
+}
+
+// the pixel view a fit call reads in ROI mode
+struct RoiView {
+    const int *slot;
+    const uint16_t *stack;
+    int side, slots;
+};
+
 }  // namespace
 
 struct loc_ctx {
     int device = 0;
     DevBuf scratch;
     // device copies for the host-buffer path
-    DevBuf frames, cands, out, flags;
+    DevBuf frames, cands, out, flags, roi_slot;
+    HostBuf pin_roi, pin_slot;   // ROI-mode staging of loc_fit_host
+    unsigned long long h2d_bytes = 0, d2h_bytes = 0;   // copied by host-buffer calls
     unsigned long long *stats_dev = nullptr;  // points into scratch of the last call
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t ev_prop = nullptr;
@@ -87,7 +221,8 @@ struct loc_ctx {
     // for uploads, fits and downloads, so that a call's upload runs while the
     // previous call fits and its download while the next call fits
     struct HostSlot {
-        DevBuf frames, cands, out, flags;
+        DevBuf frames, cands, out, flags, roi_slot;
+        HostBuf pin_roi, pin_slot;   // ROI-mode staging
         cudaEvent_t in_done = nullptr, fit_done = nullptr, out_done = nullptr;
     } slot[2];
     int next_slot = 0;
@@ -173,6 +308,7 @@ LOC_API int loc_ctx_destroy(loc_ctx *ctx)
     ctx->cands.release();
     ctx->out.release();
     ctx->flags.release();
+    ctx->roi_slot.release();
     for (int k = 0; k < 4; ++k)
         if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
     if (ctx->ev_prop) cudaEventDestroy(ctx->ev_prop);
@@ -194,9 +330,14 @@ LOC_API int loc_ctx_destroy(loc_ctx *ctx)
         sl.cands.release();
         sl.out.release();
         sl.flags.release();
+        sl.roi_slot.release();
+        sl.pin_roi.release();
+        sl.pin_slot.release();
         for (cudaEvent_t ev : {sl.in_done, sl.fit_done, sl.out_done})
             if (ev) cudaEventDestroy(ev);
     }
+    ctx->pin_roi.release();
+    ctx->pin_slot.release();
     delete ctx;
     return LOC_OK;
 }
@@ -216,9 +357,23 @@ static int validate(const loc_ctx *ctx, const void *frames, int n_frames, int n_
     return LOC_OK;
 }
 
-LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, int n_rows, int n_cols,
-                          const loc_candidate *d_cands, int n_cands, int method, double w0, double sigma,
-                          const loc_options *opt, double *d_out, uint8_t *d_flags, void *stream)
+namespace {
+
+// ROI mode is used when the slots hold fewer bytes than this fraction of the
+// frames (the CPU gather then costs less than the bytes it saves on PCIe)
+constexpr double kRoiFraction = 0.75;
+
+bool roi_mode_allowed(int method, const loc_options &o)
+{
+    // the proposal cuts its windows from whole frames; MLEwG has its own kernel
+    return method != LOC_METHOD_MLEWG && o.proposal == nullptr && o.host_roi_mode >= 0;
+}
+
+// loc_fit_batch, or with roi set a host call's ROI-mode fit (d_frames then
+// the slot stack; n_frames, n_rows and n_cols the original stack's shape)
+int fit_impl(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, int n_rows, int n_cols,
+             const loc_candidate *d_cands, int n_cands, int method, double w0, double sigma, const loc_options *opt,
+             double *d_out, uint8_t *d_flags, void *stream, const RoiView *roi)
 {
     int rc = validate(ctx, d_frames, n_frames, n_rows, n_cols, d_cands, n_cands, method, w0, sigma, d_out, d_flags);
     if (rc) return rc;
@@ -253,6 +408,8 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     if (e != cudaSuccess) return fail(LOC_E_NOMEM, std::string("scratch allocation: ") + cudaGetErrorString(e));
     locb::Scratch s;
     locb::carve_scratch(ctx->scratch.p, method, n_cands, o.precision, rerun, &s, warm ? 1 : 0);
+    if (roi && (warm || method == LOC_METHOD_MLEWG))
+        return fail(LOC_E_UNSUPPORTED, "ROI mode: no start proposal and no MLEwG");
     locb::FitParams p{};
     p.frames = d_frames;
     p.n_frames = n_frames;
@@ -260,6 +417,12 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
     p.n_cols = n_cols;
     p.cands = d_cands;
     p.n_cands = n_cands;
+    if (roi) {
+        p.roi_slot = roi->slot;
+        p.roi_stack = roi->stack;
+        p.roi_side = roi->side;
+        p.roi_slots = roi->slots;
+    }
     p.method = method;
     p.w0 = w0;
     p.sigma = sigma;
@@ -331,6 +494,16 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
         return cuda_fail(e, "fit launch");
     }
     return LOC_OK;
+}
+
+}  // namespace
+
+LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, int n_rows, int n_cols,
+                          const loc_candidate *d_cands, int n_cands, int method, double w0, double sigma,
+                          const loc_options *opt, double *d_out, uint8_t *d_flags, void *stream)
+{
+    return fit_impl(ctx, d_frames, n_frames, n_rows, n_cols, d_cands, n_cands, method, w0, sigma, opt, d_out, d_flags,
+                    stream, nullptr);
 }
 
 namespace {
@@ -547,23 +720,45 @@ LOC_API int loc_fit_host(loc_ctx *ctx, const uint16_t *frames, int n_frames, int
     if ((rc = loc_fit_host_wait(ctx)) != LOC_OK) return rc;
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
-    const size_t fbytes = (size_t)n_frames * n_rows * n_cols * sizeof(uint16_t);
+    loc_options o;
+    if (opt) o = *opt;
+    else loc_default_options(&o);
     const size_t cbytes = (size_t)n_cands * sizeof(loc_candidate);
     const int ncol = loc_output_columns(method);
     const size_t obytes = (size_t)n_cands * ncol * sizeof(double);
+    // ROI mode when the candidates' ROIs are a small part of the frames
+    RoiPlan plan;
+    if (roi_mode_allowed(method, o) && n_cands > 0) {
+        if ((e = ctx->pin_slot.ensure(sizeof(int) * (size_t)n_cands)) != cudaSuccess)
+            return fail(LOC_E_NOMEM, std::string("ROI staging: ") + cudaGetErrorString(e));
+        plan = plan_and_gather_rois(frames, n_frames, n_rows, n_cols, cands, n_cands, w0, o.max_half_width,
+                                    kRoiFraction, (int *)ctx->pin_slot.p, &ctx->pin_roi, &e);
+        if (e != cudaSuccess) return fail(LOC_E_NOMEM, std::string("ROI staging: ") + cudaGetErrorString(e));
+    }
+    const size_t fbytes = plan.use ? (size_t)plan.slots * plan.side * plan.side * sizeof(uint16_t)
+                                   : (size_t)n_frames * n_rows * n_cols * sizeof(uint16_t);
+    const size_t sbytes = plan.use ? sizeof(int) * (size_t)n_cands : 0;
     if ((e = ctx->frames.ensure(fbytes ? fbytes : 1)) != cudaSuccess ||
         (e = ctx->cands.ensure(cbytes ? cbytes : 1)) != cudaSuccess ||
         (e = ctx->out.ensure(obytes ? obytes : 1)) != cudaSuccess ||
-        (e = ctx->flags.ensure(n_cands ? n_cands : 1)) != cudaSuccess)
+        (e = ctx->flags.ensure(n_cands ? n_cands : 1)) != cudaSuccess ||
+        (e = ctx->roi_slot.ensure(sbytes ? sbytes : 1)) != cudaSuccess)
         return fail(LOC_E_NOMEM, std::string("device buffers: ") + cudaGetErrorString(e));
     cudaStream_t st = 0;
-    if (fbytes && (e = cudaMemcpyAsync(ctx->frames.p, frames, fbytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    const void *fsrc = plan.use ? ctx->pin_roi.p : (const void *)frames;
+    if (fbytes && (e = cudaMemcpyAsync(ctx->frames.p, fsrc, fbytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
         return cuda_fail(e, "frames upload");
     if (cbytes && (e = cudaMemcpyAsync(ctx->cands.p, cands, cbytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
         return cuda_fail(e, "candidates upload");
-    rc = loc_fit_batch(ctx, (const uint16_t *)ctx->frames.p, n_frames, n_rows, n_cols,
-                       (const loc_candidate *)ctx->cands.p, n_cands, method, w0, sigma, opt, (double *)ctx->out.p,
-                       (uint8_t *)ctx->flags.p, st);
+    if (sbytes &&
+        (e = cudaMemcpyAsync(ctx->roi_slot.p, ctx->pin_slot.p, sbytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return cuda_fail(e, "ROI slots upload");
+    ctx->h2d_bytes += fbytes + cbytes + sbytes;
+    ctx->d2h_bytes += obytes + (size_t)n_cands;
+    const RoiView view{(const int *)ctx->roi_slot.p, (const uint16_t *)ctx->frames.p, plan.side, plan.slots};
+    rc = fit_impl(ctx, (const uint16_t *)ctx->frames.p, n_frames, n_rows, n_cols, (const loc_candidate *)ctx->cands.p,
+                  n_cands, method, w0, sigma, opt, (double *)ctx->out.p, (uint8_t *)ctx->flags.p, st,
+                  plan.use ? &view : nullptr);
     if (rc) return rc;
     if (obytes && (e = cudaMemcpyAsync(out, ctx->out.p, obytes, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return cuda_fail(e, "rows download");
@@ -590,40 +785,61 @@ LOC_API int loc_fit_host_async(loc_ctx *ctx, const uint16_t *frames, int n_frame
                     return cuda_fail(e, "event");
     }
     loc_ctx::HostSlot &sl = ctx->slot[ctx->next_slot];
-    const size_t fbytes = (size_t)n_frames * n_rows * n_cols * sizeof(uint16_t);
     const size_t cbytes = (size_t)n_cands * sizeof(loc_candidate);
     const int ncol = loc_output_columns(method);
     const size_t obytes = (size_t)n_cands * ncol * sizeof(double);
     loc_options o;
     if (opt) o = *opt;
     else loc_default_options(&o);
+    // ROI mode: the slot's staging buffers are refilled once its previous
+    // upload has left them (the gather runs while earlier calls fit)
+    RoiPlan plan;
+    if (roi_mode_allowed(method, o) && n_cands > 0) {
+        if ((e = cudaEventSynchronize(sl.in_done)) != cudaSuccess) return cuda_fail(e, "staging wait");
+        if ((e = sl.pin_slot.ensure(sizeof(int) * (size_t)n_cands)) != cudaSuccess)
+            return fail(LOC_E_NOMEM, std::string("ROI staging: ") + cudaGetErrorString(e));
+        plan = plan_and_gather_rois(frames, n_frames, n_rows, n_cols, cands, n_cands, w0, o.max_half_width,
+                                    kRoiFraction, (int *)sl.pin_slot.p, &sl.pin_roi, &e);
+        if (e != cudaSuccess) return fail(LOC_E_NOMEM, std::string("ROI staging: ") + cudaGetErrorString(e));
+    }
+    const size_t fbytes = plan.use ? (size_t)plan.slots * plan.side * plan.side * sizeof(uint16_t)
+                                   : (size_t)n_frames * n_rows * n_cols * sizeof(uint16_t);
+    const size_t sbytes = plan.use ? sizeof(int) * (size_t)n_cands : 0;
     const size_t need = locb::scratch_bytes(method, n_cands, o.precision, o.fp64_rerun >= 0 ? 1 : 0,
                                             o.proposal ? 1 : 0);
     if (sl.frames.cap < fbytes || sl.cands.cap < cbytes || sl.out.cap < obytes || sl.flags.cap < (size_t)n_cands ||
-        ctx->scratch.cap < need) {
+        sl.roi_slot.cap < sbytes || ctx->scratch.cap < need) {
         // a buffer grows: the calls in flight may still use the old one
         if ((rc = loc_fit_host_wait(ctx)) != LOC_OK) return rc;
         if ((e = sl.frames.ensure(fbytes ? fbytes : 1)) != cudaSuccess ||
             (e = sl.cands.ensure(cbytes ? cbytes : 1)) != cudaSuccess ||
             (e = sl.out.ensure(obytes ? obytes : 1)) != cudaSuccess ||
-            (e = sl.flags.ensure(n_cands ? n_cands : 1)) != cudaSuccess)
+            (e = sl.flags.ensure(n_cands ? n_cands : 1)) != cudaSuccess ||
+            (e = sl.roi_slot.ensure(sbytes ? sbytes : 1)) != cudaSuccess)
             return fail(LOC_E_NOMEM, std::string("device buffers: ") + cudaGetErrorString(e));
     }
     // this slot's previous fit has read its frames and candidates
     if ((e = cudaStreamWaitEvent(ctx->s_in, sl.fit_done, 0)) != cudaSuccess) return cuda_fail(e, "stream wait");
-    if (fbytes && (e = cudaMemcpyAsync(sl.frames.p, frames, fbytes, cudaMemcpyHostToDevice, ctx->s_in)) != cudaSuccess)
+    const void *fsrc = plan.use ? sl.pin_roi.p : (const void *)frames;
+    if (fbytes && (e = cudaMemcpyAsync(sl.frames.p, fsrc, fbytes, cudaMemcpyHostToDevice, ctx->s_in)) != cudaSuccess)
         return cuda_fail(e, "frames upload");
     if (cbytes && (e = cudaMemcpyAsync(sl.cands.p, cands, cbytes, cudaMemcpyHostToDevice, ctx->s_in)) != cudaSuccess)
         return cuda_fail(e, "candidates upload");
+    if (sbytes && (e = cudaMemcpyAsync(sl.roi_slot.p, sl.pin_slot.p, sbytes, cudaMemcpyHostToDevice, ctx->s_in)) !=
+                      cudaSuccess)
+        return cuda_fail(e, "ROI slots upload");
     if ((e = cudaEventRecord(sl.in_done, ctx->s_in)) != cudaSuccess) return cuda_fail(e, "event record");
+    ctx->h2d_bytes += fbytes + cbytes + sbytes;
+    ctx->d2h_bytes += obytes + (size_t)n_cands;
     // the fit waits for its upload and for the download of this slot's previous rows
     if ((e = cudaStreamWaitEvent(ctx->s_fit, sl.in_done, 0)) != cudaSuccess ||
         (e = cudaStreamWaitEvent(ctx->s_fit, sl.out_done, 0)) != cudaSuccess)
         return cuda_fail(e, "stream wait");
+    const RoiView view{(const int *)sl.roi_slot.p, (const uint16_t *)sl.frames.p, plan.side, plan.slots};
     if (n_cands > 0)
-        rc = loc_fit_batch(ctx, (const uint16_t *)sl.frames.p, n_frames, n_rows, n_cols,
-                           (const loc_candidate *)sl.cands.p, n_cands, method, w0, sigma, opt, (double *)sl.out.p,
-                           (uint8_t *)sl.flags.p, ctx->s_fit);
+        rc = fit_impl(ctx, (const uint16_t *)sl.frames.p, n_frames, n_rows, n_cols, (const loc_candidate *)sl.cands.p,
+                      n_cands, method, w0, sigma, opt, (double *)sl.out.p, (uint8_t *)sl.flags.p, ctx->s_fit,
+                      plan.use ? &view : nullptr);
     if ((e = cudaEventRecord(sl.fit_done, ctx->s_fit)) != cudaSuccess) return cuda_fail(e, "event record");
     if (rc) return rc;
     if ((e = cudaStreamWaitEvent(ctx->s_out, sl.fit_done, 0)) != cudaSuccess) return cuda_fail(e, "stream wait");
@@ -633,6 +849,14 @@ LOC_API int loc_fit_host_async(loc_ctx *ctx, const uint16_t *frames, int n_frame
         return cuda_fail(e, "flags download");
     if ((e = cudaEventRecord(sl.out_done, ctx->s_out)) != cudaSuccess) return cuda_fail(e, "event record");
     ctx->next_slot ^= 1;
+    return LOC_OK;
+}
+
+LOC_API int loc_host_bytes(const loc_ctx *ctx, uint64_t *h2d, uint64_t *d2h)
+{
+    if (!ctx) return fail(LOC_E_INVALID, "ctx is NULL");
+    if (h2d) *h2d = ctx->h2d_bytes;
+    if (d2h) *d2h = ctx->d2h_bytes;
     return LOC_OK;
 }
 

@@ -28,6 +28,7 @@ struct Scratch {
     int *meta3;          // kMetaInts: its class table
     double *state64;     // n * state_stride(method): FP64 state of re-run fits
     float *init;         // n * P: proposed starts (warm mode only)
+    void *qrec;          // n start records (QRec, 48 bytes) in the order of `order`
 };
 
 constexpr int kMetaInts = 8 + 8 * (kMaxHalfWidth + 1);
@@ -78,6 +79,14 @@ struct FitParams {
     cudaEvent_t join_long[kMaxAux];
     double *out;
     uint8_t *flags;
+    // ROI mode (host-buffer calls): the pixels are not whole frames but one
+    // roi_side x roi_side slot per candidate, candidate i's ROI in slot
+    // roi_slot[i] with its origin at the slot's first pixel (roi_slot NULL:
+    // frame mode). Frames, n_frames, n_rows and n_cols above still describe
+    // the original stack (the edge and input rules use them).
+    const int *roi_slot;
+    const uint16_t *roi_stack;
+    int roi_side, roi_slots;
 };
 
 int state_stride(int method);
