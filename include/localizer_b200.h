@@ -130,8 +130,7 @@ typedef struct loc_options {
                                   re-run in FP64, iterations and status of the
                                   FP32 run, reserved */
     int32_t threads_per_fit;   /* threads cooperating on one fit in the first
-                                  scheduling level: 1 (default), 4, 8, 16 or 32
-                                  (a warp per fit) */
+                                  scheduling level: 1 (default), 4, 8 or 16 */
     int32_t tail_threads_per_fit; /* threads per fit for fits that outlive the
                                   first level's budget: 8 (default), 4 or 1 */
     int32_t level0_budget;     /* solver iterations a fit may use in the first

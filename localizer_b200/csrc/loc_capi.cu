@@ -458,10 +458,9 @@ int fit_impl(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, int n_rows, i
     if (!(p.long_rerun_threads_per_fit == 1 || p.long_rerun_threads_per_fit == 2 ||
           p.long_rerun_threads_per_fit == 4 || p.long_rerun_threads_per_fit == 8))
         return fail(LOC_E_INVALID, "long_rerun_threads_per_fit must be 1, 2, 4 or 8");
-    if (!(p.threads_per_fit == 1 || p.threads_per_fit == 4 || p.threads_per_fit == 8 || p.threads_per_fit == 16 ||
-          p.threads_per_fit == 32) ||
+    if (!(p.threads_per_fit == 1 || p.threads_per_fit == 4 || p.threads_per_fit == 8 || p.threads_per_fit == 16) ||
         !(p.tail_threads_per_fit == 1 || p.tail_threads_per_fit == 4 || p.tail_threads_per_fit == 8))
-        return fail(LOC_E_INVALID, "threads per fit must be 1, 4, 8, 16 or 32 (second level: 1, 4 or 8)");
+        return fail(LOC_E_INVALID, "threads per fit must be 1, 4, 8 or 16 (second level: 1, 4 or 8)");
     p.init_params = o.d_init_params;
     p.warm = warm;
     p.prop = prop;
@@ -572,10 +571,12 @@ LOC_API int loc_autotune(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, i
     std::vector<double> rows_ref((size_t)n_cands * ncol), rows((size_t)n_cands * ncol);
     std::vector<uint8_t> flags_ref(n_cands), flags(n_cands);
     int trials = 0;
-    // median device time of three calls after one untimed call; rows and
-    // flags of the last call copied to the host
+    // median device time of three calls after one untimed call; rows, flags
+    // and the number of fits the FP32 solver finished in the last call copied
+    // to the host (a shape must finish every fit: the rows alone could come
+    // from solver state an earlier call left in the scratch)
     auto time_shape = [&](const loc_ctx::Shape &sh, float *ms, std::vector<double> &r,
-                          std::vector<uint8_t> &f) -> int {
+                          std::vector<uint8_t> &f, unsigned long long *fits) -> int {
         loc_options o = b;
         o.threads_per_fit = sh.tpf;
         o.tail_threads_per_fit = sh.tail_tpf;
@@ -601,20 +602,22 @@ LOC_API int loc_autotune(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, i
         ++trials;
         cudaError_t e2 = cudaMemcpy(r.data(), out.p, sizeof(double) * r.size(), cudaMemcpyDeviceToHost);
         if (e2 == cudaSuccess) e2 = cudaMemcpy(f.data(), flg.p, f.size(), cudaMemcpyDeviceToHost);
+        if (e2 == cudaSuccess) e2 = cudaMemcpy(fits, ctx->stats_dev + 4, sizeof(*fits), cudaMemcpyDeviceToHost);
         if (e2 != cudaSuccess) return cuda_fail(e2, "tuning rows");
         return LOC_OK;
     };
     loc_ctx::Shape best;   // the built-in defaults
     float best_ms = 0.0f;
     long worst_flag = 0, worst_pos = 0;
-    rc = time_shape(best, &best_ms, rows_ref, flags_ref);
+    unsigned long long fits_ref = 0, fits = 0;
+    rc = time_shape(best, &best_ms, rows_ref, flags_ref, &fits_ref);
     const float ms_default = best_ms;
     // coordinate descent: each knob in turn over its values, the others held
     // at the best shape so far; a value must be 1 % faster and give the
     // default shape's results
     const std::vector<std::pair<int loc_ctx::Shape::*, std::vector<int>>> knobs = {
         {&loc_ctx::Shape::tpb, {128, 96, 64}},
-        {&loc_ctx::Shape::tpf, {1, 4, 8, 16, 32}},
+        {&loc_ctx::Shape::tpf, {1, 4, 8, 16}},
         {&loc_ctx::Shape::budget, {16, 24, 32, 48, 64}},
         {&loc_ctx::Shape::tail_tpf, {8, 4}},
         {&loc_ctx::Shape::rerun_tpf, {2, 1, 4, 8}},
@@ -627,10 +630,10 @@ LOC_API int loc_autotune(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, i
             loc_ctx::Shape trial = best;
             trial.*(kn.first) = v;
             float ms = 0.0f;
-            rc = time_shape(trial, &ms, rows, flags);
+            rc = time_shape(trial, &ms, rows, flags, &fits);
             if (rc != LOC_OK) break;
             long nf = 0, np = 0;
-            const bool same = same_results(rows, flags, rows_ref, flags_ref, ncol, xcol, &nf, &np);
+            const bool same = fits == fits_ref && same_results(rows, flags, rows_ref, flags_ref, ncol, xcol, &nf, &np);
             if (same && ms < 0.99f * best_ms) {
                 best = trial;
                 best_ms = ms;

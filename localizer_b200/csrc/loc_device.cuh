@@ -26,16 +26,6 @@ struct Cand {
 };
 static_assert(sizeof(Cand) == 40, "candidate layout");
 
-// Start record of a queued fit, in queue order (k0_scatter writes one per
-// queue slot): what the solver needs to start the fit, 16-byte aligned so
-// that the solver can prefetch it into shared memory with cp.async.
-struct alignas(16) QRec {
-    double x, y, intensity, background;
-    int frame;
-    int cand;         // candidate index: the fit's output row
-    long long base;   // pixel offset of the ROI's origin in the pixel array the solver reads
-};
-static_assert(sizeof(QRec) == 48, "start record layout");
 
 // Parameter vectors per method (reference Localization.cpp:138-142, 318-321,
 // 485-491): symmetric (A, s, x0, y0, b); fixed width (A, x0, y0, b);

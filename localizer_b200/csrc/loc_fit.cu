@@ -121,8 +121,7 @@ __global__ void k0_classes(int *meta)
     meta[M_MAXR] = maxr;
 }
 
-__global__ void k0_scatter(const int *cls, int n, int *meta, int *order, const Cand *cands, QRec *qrec,
-                           long long frame_px, int pitch, const int *roi_slot)
+__global__ void k0_scatter(const int *cls, int n, int *meta, int *order)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int c = i < n ? cls[i] : -1;
@@ -135,21 +134,7 @@ __global__ void k0_scatter(const int *cls, int n, int *meta, int *order, const C
     int base = 0;
     if (lane == leader) base = atomicAdd(&meta[m_fill(c)], __popc(peers));
     base = __shfl_sync(peers, base, leader);
-    const int pos = base + __popc(peers & ((1u << lane) - 1));
-    order[pos] = i;
-    const Cand cd = cands[i];
-    QRec q;
-    q.x = cd.x;
-    q.y = cd.y;
-    q.intensity = cd.intensity;
-    q.background = cd.background;
-    q.frame = cd.frame;
-    q.cand = i;
-    // the ROI origin: (floor(x - r), floor(y - r)) of its frame, or its slot
-    q.base = roi_slot ? (long long)roi_slot[i] * frame_px
-                      : (long long)cd.frame * frame_px + (long long)floor(cd.x - (double)c) +
-                            (long long)floor(cd.y - (double)c) * pitch;
-    qrec[pos] = q;
+    order[base + __popc(peers & ((1u << lane) - 1))] = i;
 }
 
 // Fits of the FP32 solver whose result could depend on its rounding go to an
@@ -283,11 +268,6 @@ struct K1Args {
     float *cont_state;  // saved solver state of suspended fits
     int cont_stride;
     int compensated;    // FP32 solver: sum the group's partial normal equations in FP64
-    // start records of the level-0 queue in queue order (nullptr for the
-    // continuation and re-run queues, whose fits are found through their
-    // candidate indices)
-    const QRec *qrec;
-    int n_frames;       // frames (or ROI slots) in the pixel array
     const int *roi_slot;  // ROI mode: slot of each candidate (frame_px = slot pixels, n_rows = slot side)
 };
 
@@ -362,34 +342,6 @@ template <int P> struct ContLayout {
 template <typename T>
 __host__ __device__ constexpr int state_smem_per_fit(int P) { return sizeof(T) == 8 ? (3 * tri(P) + 5 * P) * 8 : 0; }
 
-// Byte offset of the start-record slots (one QRec per fit) in the solver
-// block's shared memory: after the ROIs and the FP64 state slots, each area
-// rounded up to 16 bytes.
-template <typename T>
-__host__ __device__ constexpr int rec_smem_offset(int fits, int roi_stride_words, int P)
-{
-    return (fits * roi_stride_words * (int)sizeof(float) + 15) / 16 * 16 +
-           (fits * state_smem_per_fit<T>(P) + 15) / 16 * 16;
-}
-
-__device__ __forceinline__ void cp_async16(void *dst_smem, const void *src)
-{
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-// Bring [p, p + bytes) into L2 (p and bytes multiples of 16); a hint, no data
-// is returned
-__device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes)
-{
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
-}
-
-#ifndef LOC_ROI_L2_PREFETCH
-#define LOC_ROI_L2_PREFETCH 1
-#endif
-
 // Process one queue of ROI half-width r: the fresh candidates (level 0) or
 // the fits suspended there (level 1). TPF threads cooperate on each fit;
 // S = 2r + 1 at compile time, or 0 for a runtime side.
@@ -427,55 +379,6 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
         sstate = (T *)((char *)smem + ((roi_bytes + 15) / 16) * 16) +
                  (tid / TPF) * (state_smem_per_fit<T>(P) / (int)sizeof(T));
     }
-    // level 0 with start records: each group holds a reservation -- the
-    // queue slot of its next fit, whose record has been copied (cp.async)
-    // into the group's record slot -- taken from the warp's pool of claimed
-    // slots, which grows by one atomic per chunk of 32 / TPF slots; the
-    // queue atomic, the index and the candidate load leave the refill's
-    // critical path
-    // (FP32 with one thread per fit only: the other instantiations keep
-    // their registers for the solver)
-    constexpr bool kPref = sizeof(T) == 4 && TPF == 1;
-    const bool pref = kPref && !cont && a.qrec != nullptr;
-    QRec *myrec = (QRec *)((char *)smem + rec_smem_offset<T>(blockDim.x / TPF, stride, P)) + tid / TPF;
-    const QRec *qrec = a.qrec + cstart;
-    constexpr int kChunk = 32 / TPF;
-    int pool_next = 0, pool_end = 0;   // warp-uniform: claimed, unreserved slots [pool_next, pool_end)
-    bool pool_dry = false;             // warp-uniform: the queue has no slots left to claim
-    int res_slot = -1;                 // this group's reservation (-1: none, the queue is used up)
-    bool pf_roi = false;               // leader: the reserved fit's ROI rows are still to be sent to L2
-    // new reservations for the groups whose leader lanes are in `took`
-    auto reserve = [&](unsigned took) {
-        const int k = __popc(took);
-        const int avail = pool_end - pool_next;
-        int base = 0;
-        const bool claim = k > avail && !pool_dry;
-        if (claim) {
-            if (lane == 0) base = atomicAdd(next, kChunk);
-            base = __shfl_sync(kFull, base, 0);
-        }
-        if ((took >> glead) & 1u) {
-            const int rank = __popc(took & ((1u << glead) - 1));
-            int slot = rank < avail ? pool_next + rank : (claim ? base + (rank - avail) : -1);
-            if (slot >= ccount) slot = -1;
-            res_slot = slot;
-            if (leader && slot >= 0) {
-                const char *src = (const char *)(qrec + slot);
-#pragma unroll
-                for (int c = 0; c < 3; ++c) cp_async16((char *)myrec + 16 * c, src + 16 * c);
-                cp_async_commit();
-                pf_roi = LOC_ROI_L2_PREFETCH != 0;
-            }
-        }
-        if (claim) {
-            pool_next = base + (k - avail);
-            pool_end = base + kChunk;
-            if (pool_end >= ccount) pool_dry = true;
-        } else {
-            pool_next += k < avail ? k : avail;
-        }
-    };
-    if (pref) reserve(__ballot_sync(kFull, leader));
     // FP64: the normal equations, parameters, scaling, last step and the
     // scaled matrix of the damped solve live in the fit's shared-memory slot
     // (in registers they push the FP64 solver into spills); te, the
@@ -611,73 +514,28 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
         acc_c += (unsigned long long)(t - t_mark);
         t_mark = t;
     };
-    const char *frames_end = (const char *)(a.frames + (size_t)a.frame_px * (size_t)a.n_frames);
     while (true) {
         flush();
-        if (kPref && pf_roi && phase != 0) {
-            // a trip after the reservation its record has landed: send the
-            // reserved fit's ROI rows to L2, so that its staging at the next
-            // refill reads L2 instead of HBM
-            pf_roi = false;
-            cp_async_wait_all();
-            const char *row0 = (const char *)(a.frames + myrec->base);
-            const size_t pitch = (size_t)a.n_rows * sizeof(uint16_t);
-            for (int j = 0; j < s; ++j) {
-                const char *b = row0 + j * pitch;
-                const char *lo = (const char *)((uintptr_t)b & ~(uintptr_t)15);
-                const char *hi = (const char *)(((uintptr_t)(b + 2 * s) + 15) & ~(uintptr_t)15);
-                if (hi > frames_end) hi = (const char *)((uintptr_t)frames_end & ~(uintptr_t)15);
-                if (hi > lo) prefetch_l2(lo, (unsigned)(hi - lo));
-            }
-        }
         // ---- refill idle groups from the queue: one atomic per warp ----
         const bool want = (phase == 0) && !exhausted;
         const unsigned need = __ballot_sync(kFull, want && leader);
         if (need) {
+            const int first = __ffs(need) - 1;
+            int base = 0;
+            if (lane == first) base = atomicAdd(next, __popc(need));
+            base = __shfl_sync(kFull, base, first);
             int my = -1;
-            double cx = 0.0, cy = 0.0, cint = 0.0, cbg = 0.0;
-            int fr = 0;
-            long long rbase = 0;   // pixel offset of the ROI origin
-            if (pref) {
-                // take the reservation: its record is in the group's slot
-                if (leader) cp_async_wait_all();
-                __syncwarp();
-                if (want) {
-                    if (res_slot >= 0) {
-                        const QRec rc = *myrec;
-                        my = rc.cand;
-                        fr = rc.frame;
-                        cx = rc.x;
-                        cy = rc.y;
-                        cint = rc.intensity;
-                        cbg = rc.background;
-                        rbase = rc.base;
-                    } else {
-                        exhausted = true;
-                    }
-                }
-                __syncwarp();
-                reserve(__ballot_sync(kFull, want && leader && my >= 0));
-            } else {
-                const int first = __ffs(need) - 1;
-                int base = 0;
-                if (lane == first) base = atomicAdd(next, __popc(need));
-                base = __shfl_sync(kFull, base, first);
-                if (want) {
-                    const int qi = base + __popc(need & ((1u << glead) - 1));
-                    if (qi < ccount) my = queue[cstart + qi];
-                    else exhausted = true;
-                }
-                if (my >= 0) {
-                    const Cand cd = a.cands[my];
-                    fr = cd.frame;
-                    cx = cd.x;
-                    cy = cd.y;
-                    cint = cd.intensity;
-                    cbg = cd.background;
-                }
+            if (want) {
+                const int qi = base + __popc(need & ((1u << glead) - 1));
+                if (qi < ccount) my = queue[cstart + qi];
+                else exhausted = true;
             }
+            int fr = 0;
+            long long rbase = 0;   // pixel offset of the ROI origin in the pixel array
             if (my >= 0) {
+                const Cand cd = a.cands[my];
+                const double cx = cd.x, cy = cd.y, cint = cd.intensity, cbg = cd.background;
+                fr = cd.frame;
                 cidx = my;
                 if (cont) {
                     const float *o = a.cont_state + (size_t)my * a.cont_stride;
@@ -729,9 +587,8 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
                     }
                     phase = 1;
                 }
-                if (!pref)
-                    rbase = a.roi_slot ? (long long)a.roi_slot[my] * a.frame_px
-                                       : (long long)fr * a.frame_px + xo + (long long)yo * a.n_rows;
+                rbase = a.roi_slot ? (long long)a.roi_slot[my] * a.frame_px
+                                   : (long long)fr * a.frame_px + xo + (long long)yo * a.n_rows;
             }
             // warp-cooperative ROI staging: global uint16 -> shared float
             unsigned got = __ballot_sync(kFull, my >= 0 && leader);
@@ -751,9 +608,7 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
         // fits resumed from level 0 and fits whose last step was accepted
         // start their next outer iteration here (one inlined copy of it)
         if (phase == 3) start_iteration();
-        // a group that went idle just now (suspended at the budget, or done)
-        // may hold a reservation: it refills once more before the warp leaves
-        if (__ballot_sync(kFull, phase != 0 || (pref && !exhausted)) == 0) break;
+        if (__ballot_sync(kFull, phase != 0) == 0) break;
         lap(c_refill);
 
         // ---- choose this fit's evaluation point (identical in every sub-lane) ----
@@ -974,8 +829,6 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
         lap(c_decide);
     }
     flush();
-    // no copy into this block's shared memory outlives it
-    if (kPref) cp_async_wait_all();
     if (lane == 0) {
         st[ST_CYC_REFILL] += (unsigned)(c_refill >> 10);
         st[ST_CYC_STEP] += (unsigned)(c_step >> 10);
@@ -991,7 +844,7 @@ __host__ __device__ constexpr int k1_min_blocks(int method, int bytes) { return 
 template <int METHOD, typename T, int S, int TPF, bool ESC>
 __global__ void __launch_bounds__(128, k1_min_blocks(METHOD, sizeof(T))) k1_lm_fit(K1Args a, int r)
 {
-    extern __shared__ __align__(16) float smem[];
+    extern __shared__ float smem[];
     unsigned st[ST_N];
 #pragma unroll
     for (int k = 0; k < ST_N; ++k) st[k] = 0;
@@ -1261,12 +1114,9 @@ cudaError_t launch_k1_s(const K1Args &ka, int r, int tpb, int bps_req, cudaStrea
 {
     auto kern = k1_lm_fit<METHOD, T, S, TPF, ESC>;
     const int side = 2 * r + 1;
-    const int roi_words = roi_stride(side * side, TPF);
+    const int per_fit = roi_stride(side * side, TPF) * (int)sizeof(float);
     constexpr int P = Traits<METHOD>::P;
-    // ROIs, FP64 state slots, start-record slots (the FP32 one-thread-per-fit
-    // solver only)
-    constexpr int rec_bytes = sizeof(T) == 4 && TPF == 1 ? (int)sizeof(QRec) : 0;
-    auto smem_of = [&](int t) { return rec_smem_offset<T>(t / TPF, roi_words, P) + (t / TPF) * rec_bytes; };
+    auto smem_of = [&](int t) { return ((t / TPF) * per_fit + 15) / 16 * 16 + (t / TPF) * state_smem_per_fit<T>(P); };
     // fewer threads per block when the block's shared memory would exceed 227 KB
     while (tpb > 32 && smem_of(tpb) > 227 * 1024) tpb -= 32;
     const int smem = smem_of(tpb);
@@ -1320,9 +1170,8 @@ cudaError_t launch_k1(const K1Args &ka, int r, int tpb, int bps_req, int tpf, cu
         switch (tpf) {
         case 4: return launch_k1_tpf<METHOD, T, 4>(ka, r, tpb, bps_req, stream);
         case 8: return launch_k1_tpf<METHOD, T, 8>(ka, r, tpb, bps_req, stream);
-        // a half warp or a whole warp per fit (runtime ROI side only)
+        // a half warp per fit (runtime ROI side only)
         case 16: return launch_k1_s<METHOD, T, 0, 16>(ka, r, tpb, bps_req, stream);
-        case 32: return launch_k1_s<METHOD, T, 0, 32>(ka, r, tpb, bps_req, stream);
         default: return launch_k1_tpf<METHOD, T, 1>(ka, r, tpb, bps_req, stream);
         }
     }
@@ -1358,7 +1207,6 @@ size_t scratch_bytes(int method, int n, int precision, int rerun, int warm)
         b += al256(sizeof(int) * (size_t)n) * 3 + al256(sizeof(int) * kMetaInts) * 2 +
              al256(sizeof(double) * (size_t)n * state_stride(method));
     if (warm) b += al256(sizeof(float) * (size_t)n * 8);
-    b += al256(sizeof(QRec) * (size_t)n);
     return b;
 }
 
@@ -1398,8 +1246,6 @@ void carve_scratch(void *base, int method, int n, int precision, int rerun, Scra
         s->state64 = nullptr;
     }
     s->init = warm ? (float *)p : nullptr;
-    if (warm) p += al256(sizeof(float) * (size_t)n * 8);
-    s->qrec = (void *)p;
 }
 
 namespace {
@@ -1472,15 +1318,13 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
     const uint16_t *px = roi_mode ? p.roi_stack : p.frames;
     const long long px_frame = roi_mode ? (long long)p.roi_side * p.roi_side : (long long)p.n_rows * p.n_cols;
     const int px_pitch = roi_mode ? p.roi_side : p.n_rows;
-    const int px_frames = roi_mode ? p.roi_slots : p.n_frames;
     K0Args k0{(const Cand *)p.cands, n, p.n_frames, p.n_rows, p.n_cols, r_default, r_cap, p.method, ncol_total,
               p.out, p.flags, s.cls, s.meta, rerun ? s.cls2 : nullptr, p.roi_slot, p.roi_slots,
               (p.roi_side - 1) / 2};
     const int nb = (n + 255) / 256;
     k0_classify<<<nb, 256, 0, stream>>>(k0);
     k0_classes<<<1, 32, 0, stream>>>(s.meta);
-    k0_scatter<<<nb, 256, 0, stream>>>(s.cls, n, s.meta, s.order, (const Cand *)p.cands, (QRec *)s.qrec, px_frame,
-                                       px_pitch, p.roi_slot);
+    k0_scatter<<<nb, 256, 0, stream>>>(s.cls, n, s.meta, s.order);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     bump();
     bump();
@@ -1513,8 +1357,7 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
               s.state, state_stride(p.method), (float)p.w0, (float)(1.0 / (p.sigma * p.sigma)),
               (float)(1.0 / s_abs), 1.0 / (p.sigma * p.sigma), 1.0 / s_abs, p.max_iter, (float)p.epsabs,
               (float)p.epsrel, p.precision == 1 ? 0.0f : p.pivot_thr, p.warm ? s.init : p.init_params, s.stats,
-              0, 0, s.cont, s.cont_state, cont_stride_of(m), p.compensated, (const QRec *)s.qrec, px_frames,
-              p.roi_slot};
+              0, 0, s.cont, s.cont_state, cont_stride_of(m), p.compensated, p.roi_slot};
     // Each ROI class is an independent chain -- level 0 (every candidate,
     // tpf0 threads per fit, up to `budget` iterations), level 1 (the fits
     // still running, tpf1 threads per fit), the flag pass and the FP64
@@ -1574,7 +1417,6 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
                 K1Args k64 = k1;
                 // warm-started fits fall back to the reference start
                 if (p.warm) k64.init_params = nullptr;
-                k64.qrec = nullptr;
                 k64.order = s.order2;
                 k64.meta = s.meta2;
                 k64.state = s.state64;

@@ -28,7 +28,6 @@ struct Scratch {
     int *meta3;          // kMetaInts: its class table
     double *state64;     // n * state_stride(method): FP64 state of re-run fits
     float *init;         // n * P: proposed starts (warm mode only)
-    void *qrec;          // n start records (QRec, 48 bytes) in the order of `order`
 };
 
 constexpr int kMetaInts = 8 + 8 * (kMaxHalfWidth + 1);

@@ -48,7 +48,7 @@ def test_tuned_shape_is_applied_and_keeps_results(method):
         base = L.default_options(max_half_width=6)
         t = eng.autotune(frames.data_ptr(), frames.shape[0], frames.shape[2], frames.shape[1], d_cands.data_ptr(),
                          n, method, w.w0, options=base)
-        assert t["threads_per_fit"] in (1, 4, 8, 16, 32) and t["tail_threads_per_fit"] in (4, 8)
+        assert t["threads_per_fit"] in (1, 4, 8, 16) and t["tail_threads_per_fit"] in (4, 8)
         assert t["level0_budget"] in (16, 24, 32, 48, 64) and t["threads_per_block"] in (64, 96, 128)
         assert t["rerun_threads_per_fit"] in (1, 2, 4, 8) and t["long_rerun_threads_per_fit"] in (2, 4, 8)
         assert t["trials"] >= 10 and 0 < t["ms_tuned"] <= t["ms_default"]
@@ -80,3 +80,32 @@ def test_autotune_rejects_bad_input():
     lib = L.lib()
     t = L.Tuning()
     assert lib.loc_autotune(None, None, 1, 8, 8, None, 1, 0, 1.3, 1.0, None, t, None) == -1
+
+
+@pytest.mark.parametrize("method", [0, 7])
+def test_every_shape_finishes_every_fit(method):
+    """Each shape the tuner may pick (threads per fit in either level, first-
+    level budget, FP64 re-run threads) finishes every enqueued fit, in a
+    fresh context whose scratch holds no earlier call's solver state, and
+    gives the default shape's flags for all but a handful of fits."""
+    w, frames, cands, d_cands = _workload(60)
+    n = len(cands)
+    base = L.default_options(max_half_width=6)
+    eng = L.Engine(0)
+    try:
+        rows0, flags0 = _fit(eng, frames, d_cands, n, method, w.w0, base)
+        enqueued = int(np.sum((flags0 != 1) & (flags0 != 10)))
+        assert eng.stats()["fits"] == enqueued
+    finally:
+        eng.close()
+    shapes = [dict(threads_per_fit=t, level0_budget=b) for t in (1, 4, 8, 16) for b in (16, 64)]
+    shapes += [dict(tail_threads_per_fit=4), dict(tail_threads_per_fit=1), dict(rerun_threads_per_fit=1),
+               dict(rerun_threads_per_fit=8, long_rerun_threads_per_fit=2), dict(threads_per_block=64)]
+    for kw in shapes:
+        eng = L.Engine(0)
+        try:
+            rows, flags = _fit(eng, frames, d_cands, n, method, w.w0, L.default_options(max_half_width=6, **kw))
+            assert eng.stats()["fits"] == enqueued, kw
+            assert np.sum(flags != flags0) <= max(2, n // 2000), kw
+        finally:
+            eng.close()
