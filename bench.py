@@ -652,7 +652,7 @@ def main():
                "frame_bytes_per_step": int(frames_dev.numel() * 2),
                "call": f"loc_fit_host_async per block of {blk} frames ({len(chunks)} calls per step, pinned host "
                        f"buffers, uploads overlapping the previous call's fit, ROI upload where the "
-                       f"candidates' ROIs are under 3/4 of the frames), loc_fit_host_wait at the end",
+                       f"candidates' ROIs are under half of the frames), loc_fit_host_wait at the end",
                "steps": e_steps, "ms_per_step": e_ms / e_steps}
         # the host-buffer path gives the device path's rows
         for b0, b1, lo, hi, m, pc, po, pf in chunks:

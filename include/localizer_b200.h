@@ -207,11 +207,13 @@ typedef struct loc_options {
                                   start's) */
     int32_t host_roi_mode;     /* loc_fit_host / loc_fit_host_async: 0
                                   (default): when the candidates' ROIs hold
-                                  fewer than 3/4 of the stack's pixels, only
-                                  they cross PCIe (gathered on the host into
-                                  one slot per candidate; rows identical to
-                                  the whole-frame upload); not with a proposal
-                                  or method 6; < 0: always upload whole frames */
+                                  fewer than half the stack's pixels and there
+                                  are at least 10^5 candidates, only the ROIs
+                                  cross PCIe (gathered by host threads into one
+                                  slot per candidate; rows identical to the
+                                  whole-frame upload); > 0: whenever the slots
+                                  are smaller than the frames; < 0: always
+                                  whole frames. Not with a proposal or method 6 */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */
@@ -279,8 +281,10 @@ LOC_API int loc_fit_host(loc_ctx *ctx, const uint16_t *frames, int n_frames, int
  * it (two device slots used in turn). `frames`, `cands`, `out` and `flags`
  * must stay valid, and `out`/`flags` unread, until loc_fit_host_wait
  * returns; pinned host memory (cudaHostAlloc / cudaHostRegister) is needed
- * for the copies to overlap. Make no other fit call on the context while
- * calls are in flight. Results are identical to loc_fit_host's.
+ * for the copies to overlap (in ROI mode the frames are read by the host
+ * threads during the call and the slots are copied from the library's own
+ * pinned staging). Make no other fit call on the context while calls are in
+ * flight. Results are identical to loc_fit_host's.
  */
 LOC_API int loc_fit_host_async(loc_ctx *ctx, const uint16_t *frames, int n_frames, int n_rows,
                                int n_cols, const loc_candidate *cands, int n_cands, int method,

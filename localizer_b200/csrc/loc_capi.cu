@@ -88,6 +88,14 @@ struct HostBuf {
 // holding its (2r+1)^2 ROI at the slot's origin, side = 2 rmax + 1 over the
 // call; only the slots cross PCIe. The solver reads the same pixels from the
 // slots, so the rows are those of the frame upload.
+// Automatic ROI mode needs the slots to hold fewer bytes than kRoiFraction of
+// the frames and at least kRoiMinCands candidates: otherwise the gather
+// (thread start-up, one cache miss per ROI row) costs more than the copy it
+// saves (measured: at 0.52 the gather of a single 1.8 M-candidate call took
+// longer than the whole-frame copy it replaced; at 0.43 and 0.09 it paid)
+constexpr double kRoiFraction = 0.5;
+constexpr int kRoiMinCands = 100000;
+
 struct RoiPlan {
     bool use = false;
     int slots = 0, side = 0;
@@ -103,8 +111,8 @@ int host_threads()
 // reading pixels. Gathers into roi (slots x side^2 uint16) when the slots
 // hold fewer bytes than max_fraction of the frames.
 RoiPlan plan_and_gather_rois(const uint16_t *frames, int n_frames, int n_rows, int n_cols, const loc_candidate *c,
-                             int n, double w0, int max_half_width, double max_fraction, int *slot_of,
-                             HostBuf *roi, cudaError_t *err)
+                             int n, double w0, int max_half_width, bool force, int *slot_of, HostBuf *roi,
+                             cudaError_t *err)
 {
     RoiPlan plan;
     *err = cudaSuccess;
@@ -152,26 +160,41 @@ RoiPlan plan_and_gather_rois(const uint16_t *frames, int n_frames, int n_rows, i
         total += cnt[t];
         rm = std::max(rm, rmax[t]);
     }
-    if (total == 0) return plan;
+    if (total == 0 || (!force && total < kRoiMinCands)) return plan;
     const int side = 2 * rm + 1;
     const double roi_bytes = (double)total * side * side * sizeof(uint16_t);
     const double frame_bytes = (double)n_frames * n_rows * n_cols * sizeof(uint16_t);
-    if (!(roi_bytes < max_fraction * frame_bytes)) return plan;
+    if (!(roi_bytes < (force ? 1.0 : kRoiFraction) * frame_bytes)) return plan;
     if ((*err = roi->ensure((size_t)roi_bytes)) != cudaSuccess) return plan;
     uint16_t *dst0 = (uint16_t *)roi->p;
     const size_t fpx = (size_t)n_rows * n_cols;
+    // the rows of a ROI a few candidates ahead are requested before the
+    // current ROI is copied: every row is a cache miss in another frame row,
+    // and the copy is bound by their latency, not by bandwidth
+    constexpr int kAhead = 8;
+    auto roi_src = [&](const loc_candidate &q, int &sd) {
+        const int r = q.half_width > 0 ? q.half_width : r_default;
+        sd = 2 * r + 1;
+        const size_t xo = (size_t)std::floor(q.x - (double)r), yo = (size_t)std::floor(q.y - (double)r);
+        return frames + (size_t)q.frame * fpx + xo + yo * (size_t)n_rows;
+    };
     // pass 2: slot numbers in candidate order, rows copied into the slots
     run([&](int t) {
         int lo, hi;
         chunk(t, lo, hi);
         for (int i = lo; i < hi; ++i) {
+            if (i + kAhead < hi && slot_of[i + kAhead] >= 0) {
+                int sa;
+                const uint16_t *pa = roi_src(c[i + kAhead], sa);
+                for (int j = 0; j < sa; ++j) {
+                    __builtin_prefetch(pa + (size_t)j * n_rows);
+                    __builtin_prefetch(pa + (size_t)j * n_rows + sa - 1);
+                }
+            }
             if (slot_of[i] < 0) continue;
             const int slot = (slot_of[i] += base[t]);
-            const loc_candidate &q = c[i];
-            const int r = q.half_width > 0 ? q.half_width : r_default;
-            const int sd = 2 * r + 1;
-            const size_t xo = (size_t)std::floor(q.x - (double)r), yo = (size_t)std::floor(q.y - (double)r);
-            const uint16_t *src = frames + (size_t)q.frame * fpx + xo + yo * (size_t)n_rows;
+            int sd;
+            const uint16_t *src = roi_src(c[i], sd);
             uint16_t *dst = dst0 + (size_t)slot * side * side;
             for (int j = 0; j < sd; ++j)
                 std::memcpy(dst + (size_t)j * side, src + (size_t)j * n_rows, (size_t)sd * sizeof(uint16_t));
@@ -358,10 +381,6 @@ static int validate(const loc_ctx *ctx, const void *frames, int n_frames, int n_
 }
 
 namespace {
-
-// ROI mode is used when the slots hold fewer bytes than this fraction of the
-// frames (the CPU gather then costs less than the bytes it saves on PCIe)
-constexpr double kRoiFraction = 0.75;
 
 bool roi_mode_allowed(int method, const loc_options &o)
 {
@@ -735,7 +754,7 @@ LOC_API int loc_fit_host(loc_ctx *ctx, const uint16_t *frames, int n_frames, int
         if ((e = ctx->pin_slot.ensure(sizeof(int) * (size_t)n_cands)) != cudaSuccess)
             return fail(LOC_E_NOMEM, std::string("ROI staging: ") + cudaGetErrorString(e));
         plan = plan_and_gather_rois(frames, n_frames, n_rows, n_cols, cands, n_cands, w0, o.max_half_width,
-                                    kRoiFraction, (int *)ctx->pin_slot.p, &ctx->pin_roi, &e);
+                                    o.host_roi_mode > 0, (int *)ctx->pin_slot.p, &ctx->pin_roi, &e);
         if (e != cudaSuccess) return fail(LOC_E_NOMEM, std::string("ROI staging: ") + cudaGetErrorString(e));
     }
     const size_t fbytes = plan.use ? (size_t)plan.slots * plan.side * plan.side * sizeof(uint16_t)
@@ -802,7 +821,7 @@ LOC_API int loc_fit_host_async(loc_ctx *ctx, const uint16_t *frames, int n_frame
         if ((e = sl.pin_slot.ensure(sizeof(int) * (size_t)n_cands)) != cudaSuccess)
             return fail(LOC_E_NOMEM, std::string("ROI staging: ") + cudaGetErrorString(e));
         plan = plan_and_gather_rois(frames, n_frames, n_rows, n_cols, cands, n_cands, w0, o.max_half_width,
-                                    kRoiFraction, (int *)sl.pin_slot.p, &sl.pin_roi, &e);
+                                    o.host_roi_mode > 0, (int *)sl.pin_slot.p, &sl.pin_roi, &e);
         if (e != cudaSuccess) return fail(LOC_E_NOMEM, std::string("ROI staging: ") + cudaGetErrorString(e));
     }
     const size_t fbytes = plan.use ? (size_t)plan.slots * plan.side * plan.side * sizeof(uint16_t)

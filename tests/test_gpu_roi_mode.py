@@ -49,12 +49,12 @@ def test_roi_mode_rows_match_frame_upload(engine, name, method):
     h0, _ = engine.host_bytes()
     rows_f, flags_f = engine.fit_host(frames, cands, method, w.w0, options=L.default_options(host_roi_mode=-1))
     h1, _ = engine.host_bytes()
-    rows_r, flags_r = engine.fit_host(frames, cands, method, w.w0)
+    rows_r, flags_r = engine.fit_host(frames, cands, method, w.w0, options=L.default_options(host_roi_mode=1))
     h2, _ = engine.host_bytes()
     np.testing.assert_array_equal(flags_r, flags_f)
     np.testing.assert_array_equal(rows_r, rows_f)
     assert h1 - h0 >= frames.nbytes
-    assert h2 - h1 < 0.75 * frames.nbytes + cands.nbytes + 4 * len(cands)   # ROI mode was taken
+    assert h2 - h1 < frames.nbytes + cands.nbytes + 4 * len(cands)   # ROI mode was taken
     # the rejects: edge (2), bad input (NaN, frame range, half-width above the cap)
     assert list(flags_r[-7:]) == [1, 1, 10, 1, 10, 10, 10]
 
@@ -64,7 +64,8 @@ def test_roi_mode_with_half_width_cap_and_device_call(engine):
     w, frames, cands = _stack("uneven", 16, 710)
     # a cap below some candidates' half-width: those are bad input in both modes
     opts = L.default_options(max_half_width=5)
-    rows_r, flags_r = engine.fit_host(frames, cands, 7, w.w0, options=opts)
+    rows_r, flags_r = engine.fit_host(frames, cands, 7, w.w0, options=L.default_options(max_half_width=5,
+                                                                                         host_roi_mode=1))
     rows_f, flags_f = engine.fit_host(frames, cands, 7, w.w0, options=L.default_options(max_half_width=5,
                                                                                          host_roi_mode=-1))
     np.testing.assert_array_equal(flags_r, flags_f)
@@ -88,8 +89,8 @@ def test_roi_mode_async_stream_of_stacks(engine):
     different sizes (staging buffers reused and grown while calls are in
     flight) give the synchronous whole-frame rows."""
     jobs = []
-    for name, nf, method, mode in (("stress", 20, 0, 0), ("uneven", 8, 7, 0), ("uneven", 30, 7, -1),
-                                   ("stress", 40, 0, 0), ("uneven", 12, 5, 0), ("stress", 20, 0, 0)):
+    for name, nf, method, mode in (("stress", 20, 0, 1), ("uneven", 8, 7, 1), ("uneven", 30, 7, -1),
+                                   ("stress", 40, 0, 1), ("uneven", 12, 5, 0), ("stress", 20, 0, 1)):
         w, frames, cands = _stack(name, nf, 720 + nf)
         jobs.append((w, frames, cands, method, mode))
     expect = [engine.fit_host(fr, c, m, w.w0, options=L.default_options(host_roi_mode=-1))
@@ -108,8 +109,9 @@ def test_roi_mode_async_stream_of_stacks(engine):
 
 
 def test_dense_candidates_fall_back_to_frames(engine):
-    """Candidates whose ROIs cover most of the frames: the whole frames are
-    copied (the slots would be larger)."""
+    """Candidates whose ROIs cover the frames several times over: the whole
+    frames are copied even when ROI mode is asked for (the slots would be
+    larger)."""
     w, frames, _ = _stack("small", 4, 730)
     n_frames, n_cols, n_rows = frames.shape
     ys, xs = np.meshgrid(np.arange(8, n_cols - 8, 2), np.arange(8, n_rows - 8, 2), indexing="ij")
@@ -121,7 +123,7 @@ def test_dense_candidates_fall_back_to_frames(engine):
     c["background"] = 100.0
     c["frame"] = np.repeat(np.arange(n_frames), per)
     h0, _ = engine.host_bytes()
-    rows_r, flags_r = engine.fit_host(frames, c, 0, w.w0)
+    rows_r, flags_r = engine.fit_host(frames, c, 0, w.w0, options=L.default_options(host_roi_mode=1))
     h1, _ = engine.host_bytes()
     rows_f, flags_f = engine.fit_host(frames, c, 0, w.w0, options=L.default_options(host_roi_mode=-1))
     assert h1 - h0 >= frames.nbytes
