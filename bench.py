@@ -607,10 +607,11 @@ def main():
             pf = torch.empty(hi - lo, dtype=torch.uint8, pin_memory=True)
             chunks.append((b0, b1, lo, hi, m, pc, po, pf))
         assert np.all(np.diff(fr_all) >= 0)
-        e_eng = parts[0].eng
-        # the host-buffer calls run on one context: each method's tuned
-        # launch shape is passed explicitly, so the rows match the device
-        # path's bit for bit
+        # each method's blocks go to that method's context (its own streams
+        # and staging), as in the device arm, so one method's fits overlap
+        # the other's gather and copies; each method's tuned launch shape is
+        # passed explicitly, so the rows match the device path's bit for bit
+        e_eng = {p.method: p.eng for p in parts}
         e_opts = {p.method: L.default_options(max_half_width=mh, precision=args.precision,
                                               **{k: tuned[p.method][k] for k in SHAPE_KEYS if p.method in tuned})
                   for p in parts}
@@ -618,15 +619,20 @@ def main():
 
         def e2e_step():
             for b0, b1, lo, hi, m, pc, po, pf in chunks:
-                rc = lib.loc_fit_host_async(e_eng.handle, C.c_void_p(frames_pinned.data_ptr() + b0 * fb), b1 - b0,
+                rc = lib.loc_fit_host_async(e_eng[m].handle, C.c_void_p(frames_pinned.data_ptr() + b0 * fb), b1 - b0,
                                             size, size, C.c_void_p(pc.data_ptr()), hi - lo, m, w.w0, 1.0,
                                             C.byref(e_opts[m]), C.c_void_p(po.data_ptr()), C.c_void_p(pf.data_ptr()))
                 if rc != 0:
                     raise RuntimeError(lib.loc_last_error().decode())
 
         def wait():
-            if lib.loc_fit_host_wait(e_eng.handle) != 0:
-                raise RuntimeError(lib.loc_last_error().decode())
+            for eng_m in e_eng.values():
+                if lib.loc_fit_host_wait(eng_m.handle) != 0:
+                    raise RuntimeError(lib.loc_last_error().decode())
+
+        def host_bytes():
+            hb = [eng_m.host_bytes() for eng_m in e_eng.values()]
+            return sum(h[0] for h in hb), sum(h[1] for h in hb)
 
         e_steps = args.e2e_steps or min(args.steps, 10)
         e2e_step()
@@ -636,23 +642,23 @@ def main():
             torch.distributed.barrier()
         dstream = torch.cuda.default_stream()
         s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        hb0 = e_eng.host_bytes()
+        hb0 = host_bytes()
         s2.record(dstream)
         for _ in range(e_steps):
             e2e_step()
         wait()
         e2.record(dstream)
         torch.cuda.synchronize()
-        hb1 = e_eng.host_bytes()
+        hb1 = host_bytes()
         _, e_ms, e_rate = DI.job_throughput(n * e_steps, s2.elapsed_time(e2))
         # bytes the library copied (its own count: with the ROI upload only the
         # candidates' ROIs cross PCIe, gathered on the host inside the calls)
         e2e = {"value": e_rate, "unit": UNIT, "h2d_bytes_per_step": int((hb1[0] - hb0[0]) // e_steps),
                "d2h_bytes_per_step": int((hb1[1] - hb0[1]) // e_steps), "arm": "plain",
                "frame_bytes_per_step": int(frames_dev.numel() * 2),
-               "call": f"loc_fit_host_async per block of {blk} frames ({len(chunks)} calls per step, pinned host "
-                       f"buffers, uploads overlapping the previous call's fit, ROI upload where the "
-                       f"candidates' ROIs are under half of the frames), loc_fit_host_wait at the end",
+               "call": f"loc_fit_host_async per block of {blk} frames ({len(chunks)} calls per step, one context "
+                       f"per method, pinned host buffers, uploads overlapping the previous call's fit, ROI upload "
+                       f"where the candidates' ROIs are under half of the frames), loc_fit_host_wait at the end",
                "steps": e_steps, "ms_per_step": e_ms / e_steps}
         # the host-buffer path gives the device path's rows
         for b0, b1, lo, hi, m, pc, po, pf in chunks:

@@ -210,10 +210,11 @@ typedef struct loc_options {
                                   fewer than half the stack's pixels and there
                                   are at least 10^5 candidates, only the ROIs
                                   cross PCIe (gathered by host threads into one
-                                  slot per candidate; rows identical to the
-                                  whole-frame upload); > 0: whenever the slots
-                                  are smaller than the frames; < 0: always
-                                  whole frames. Not with a proposal or method 6 */
+                                  packed stack, each ROI at its own size; rows
+                                  identical to the whole-frame upload); > 0:
+                                  whenever the stack is smaller than the
+                                  frames; < 0: always whole frames. Not with a
+                                  proposal or method 6 */
 } loc_options;
 
 /* Fills *opt with the reference's defaults. */
@@ -265,8 +266,9 @@ LOC_API int loc_fit_batch(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, 
 /* Same fit with host buffers: copies frames and candidates to the device,
  * fits and copies rows and flags back (the whole path a host caller sees).
  * Where the candidates' ROIs are a small part of the frames (host_roi_mode),
- * the host threads gather each candidate's ROI into a slot and only the
- * slots are copied; the solver reads the same pixels from them. */
+ * the host threads gather the candidates' ROIs into one packed stack and
+ * only the stack (plus one pixel offset per candidate) is copied; the solver
+ * reads the same pixels from it. */
 LOC_API int loc_fit_host(loc_ctx *ctx, const uint16_t *frames, int n_frames, int n_rows,
                          int n_cols, const loc_candidate *cands, int n_cands, int method,
                          double w0, double sigma, const loc_options *opt, double *out,
@@ -282,8 +284,8 @@ LOC_API int loc_fit_host(loc_ctx *ctx, const uint16_t *frames, int n_frames, int
  * must stay valid, and `out`/`flags` unread, until loc_fit_host_wait
  * returns; pinned host memory (cudaHostAlloc / cudaHostRegister) is needed
  * for the copies to overlap (in ROI mode the frames are read by the host
- * threads during the call and the slots are copied from the library's own
- * pinned staging). Make no other fit call on the context while calls are in
+ * threads during the call and the ROI stack is copied from the library's
+ * own pinned staging). Make no other fit call on the context while calls are in
  * flight. Results are identical to loc_fit_host's.
  */
 LOC_API int loc_fit_host_async(loc_ctx *ctx, const uint16_t *frames, int n_frames, int n_rows,

@@ -82,13 +82,14 @@ struct HostBuf {
     }
 };
 
-// ROI mode of the host-buffer calls. Instead of whole frames, each candidate
-// that the fit's input and edge rules keep (the rules of k0_classify, the
-// reference's Localization.cpp:115-124) gets a slot of side x side pixels
-// holding its (2r+1)^2 ROI at the slot's origin, side = 2 rmax + 1 over the
-// call; only the slots cross PCIe. The solver reads the same pixels from the
-// slots, so the rows are those of the frame upload.
-// Automatic ROI mode needs the slots to hold fewer bytes than kRoiFraction of
+// ROI mode of the host-buffer calls. Instead of whole frames, the (2r+1)^2
+// ROI of each candidate that the fit's input and edge rules keep (the rules
+// of k0_classify, the reference's Localization.cpp:115-124) is copied into
+// one packed stack, ROI after ROI in candidate order, each with its own row
+// pitch 2r+1; only the stack and one pixel offset per candidate cross PCIe.
+// The solver reads the same pixels from the stack, so the rows are those of
+// the frame upload.
+// Automatic ROI mode needs the stack to hold fewer bytes than kRoiFraction of
 // the frames and at least kRoiMinCands candidates: otherwise the gather
 // (thread start-up, one cache miss per ROI row) costs more than the copy it
 // saves (measured: at 0.52 the gather of a single 1.8 M-candidate call took
@@ -98,7 +99,7 @@ constexpr int kRoiMinCands = 100000;
 
 struct RoiPlan {
     bool use = false;
-    int slots = 0, side = 0;
+    long long px = 0;   // pixels in the packed stack
 };
 
 int host_threads()
@@ -107,11 +108,40 @@ int host_threads()
     return (int)std::max(1u, std::min(hc ? hc : 1u, 32u));
 }
 
-// slot_of[i]: the candidate's slot, -1 for a candidate the fit rejects before
-// reading pixels. Gathers into roi (slots x side^2 uint16) when the slots
-// hold fewer bytes than max_fraction of the frames.
+// Copies the sd x sd ROI at src (row pitch src_pitch) to dst (row pitch sd).
+// Rows of up to 16 pixels move as fixed 32-byte copies while such a copy
+// ends inside the ROI: it spills into the following destination rows, which
+// later copies overwrite. The remaining rows are copied exactly (two
+// overlapping fixed copies), so nothing past the ROI is written. end bounds
+// the source buffer.
+inline void copy_roi(uint16_t *dst, const uint16_t *src, int sd, size_t src_pitch, const uint16_t *end)
+{
+    int j = 0;
+    const int nfast = sd <= 16 && sd * sd >= 16 ? std::min(sd - 1, (sd * sd - 16) / sd + 1) : 0;
+    if (nfast > 0 && src + (size_t)(nfast - 1) * src_pitch + 16 <= end)
+        for (; j < nfast; ++j) std::memcpy(dst + (size_t)j * sd, src + (size_t)j * src_pitch, 32);
+    for (; j < sd; ++j) {
+        unsigned char *d = reinterpret_cast<unsigned char *>(dst + (size_t)j * sd);
+        const unsigned char *s = reinterpret_cast<const unsigned char *>(src + (size_t)j * src_pitch);
+        const size_t nb = (size_t)sd * sizeof(uint16_t);
+        if (nb >= 16 && nb <= 32) {
+            std::memcpy(d, s, 16);
+            std::memcpy(d + nb - 16, s + nb - 16, 16);
+        } else if (nb >= 8 && nb < 16) {
+            std::memcpy(d, s, 8);
+            std::memcpy(d + nb - 8, s + nb - 8, 8);
+        } else {
+            std::memcpy(d, s, nb);
+        }
+    }
+}
+
+// off[i]: the first pixel of the candidate's ROI in the packed stack, -1 for
+// a candidate the fit rejects before reading pixels. Gathers into roi when
+// the stack holds fewer bytes than max_fraction of the frames (and fewer
+// than 2^31 pixels, the range of the offsets).
 RoiPlan plan_and_gather_rois(const uint16_t *frames, int n_frames, int n_rows, int n_cols, const loc_candidate *c,
-                             int n, double w0, int max_half_width, bool force, int *slot_of, HostBuf *roi,
+                             int n, double w0, int max_half_width, bool force, int *off, HostBuf *roi,
                              cudaError_t *err)
 {
     RoiPlan plan;
@@ -120,7 +150,7 @@ RoiPlan plan_and_gather_rois(const uint16_t *frames, int n_frames, int n_rows, i
     const int r_default = (int)std::ceil(w0 * 4.0);
     const int r_cap = max_half_width > 0 ? std::min(max_half_width, locb::kMaxHalfWidth) : locb::kMaxHalfWidth;
     const int nt = std::min(host_threads(), std::max(1, n / 4096));
-    std::vector<int> cnt(nt, 0), rmax(nt, 0);
+    std::vector<long long> cnt(nt, 0), npx(nt, 0);
     auto chunk = [&](int t, int &lo, int &hi) {
         lo = (int)((long long)n * t / nt);
         hi = (int)((long long)n * (t + 1) / nt);
@@ -131,59 +161,63 @@ RoiPlan plan_and_gather_rois(const uint16_t *frames, int n_frames, int n_rows, i
         fn(0);
         for (auto &x : th) x.join();
     };
-    // pass 1: which candidates read pixels, and the largest ROI
+    auto half_width = [&](const loc_candidate &q) { return q.half_width > 0 ? q.half_width : r_default; };
+    // pass 1: which candidates read pixels, and each thread's pixel count
     run([&](int t) {
-        int lo, hi, k = 0, rm = 0;
+        int lo, hi;
+        long long k = 0, px = 0;
         chunk(t, lo, hi);
         for (int i = lo; i < hi; ++i) {
             const loc_candidate &q = c[i];
             const bool finite = std::isfinite(q.x) && std::isfinite(q.y) && std::isfinite(q.intensity) &&
                                 std::isfinite(q.background);
-            const int r = q.half_width > 0 ? q.half_width : r_default;
-            int slot = -1;
+            const int r = half_width(q);
+            int o = -1;
             if (finite && q.frame >= 0 && q.frame < n_frames && q.half_width >= 0 && r >= 1 && r <= r_cap) {
                 const double xo = std::floor(q.x - (double)r), yo = std::floor(q.y - (double)r);
                 if (!(xo < 0 || xo + 2 * r > n_rows - 1 || yo < 0 || yo + 2 * r > n_cols - 1)) {
-                    slot = k++;
-                    rm = std::max(rm, r);
+                    o = 0;
+                    ++k;
+                    px += (long long)(2 * r + 1) * (2 * r + 1);
                 }
             }
-            slot_of[i] = slot;
+            off[i] = o;
         }
         cnt[t] = k;
-        rmax[t] = rm;
+        npx[t] = px;
     });
-    std::vector<int> base(nt, 0);
-    int total = 0, rm = 0;
+    std::vector<long long> base(nt, 0);
+    long long total = 0, kept = 0;
     for (int t = 0; t < nt; ++t) {
         base[t] = total;
-        total += cnt[t];
-        rm = std::max(rm, rmax[t]);
+        total += npx[t];
+        kept += cnt[t];
     }
-    if (total == 0 || (!force && total < kRoiMinCands)) return plan;
-    const int side = 2 * rm + 1;
-    const double roi_bytes = (double)total * side * side * sizeof(uint16_t);
+    if (kept == 0 || (!force && kept < kRoiMinCands) || total >= (1ll << 31)) return plan;
+    const double roi_bytes = (double)total * sizeof(uint16_t);
     const double frame_bytes = (double)n_frames * n_rows * n_cols * sizeof(uint16_t);
     if (!(roi_bytes < (force ? 1.0 : kRoiFraction) * frame_bytes)) return plan;
     if ((*err = roi->ensure((size_t)roi_bytes)) != cudaSuccess) return plan;
     uint16_t *dst0 = (uint16_t *)roi->p;
     const size_t fpx = (size_t)n_rows * n_cols;
+    const uint16_t *end = frames + (size_t)n_frames * fpx;
     // the rows of a ROI a few candidates ahead are requested before the
     // current ROI is copied: every row is a cache miss in another frame row,
     // and the copy is bound by their latency, not by bandwidth
     constexpr int kAhead = 8;
     auto roi_src = [&](const loc_candidate &q, int &sd) {
-        const int r = q.half_width > 0 ? q.half_width : r_default;
+        const int r = half_width(q);
         sd = 2 * r + 1;
         const size_t xo = (size_t)std::floor(q.x - (double)r), yo = (size_t)std::floor(q.y - (double)r);
         return frames + (size_t)q.frame * fpx + xo + yo * (size_t)n_rows;
     };
-    // pass 2: slot numbers in candidate order, rows copied into the slots
+    // pass 2: offsets in candidate order, rows copied into the stack
     run([&](int t) {
         int lo, hi;
         chunk(t, lo, hi);
+        long long at = base[t];
         for (int i = lo; i < hi; ++i) {
-            if (i + kAhead < hi && slot_of[i + kAhead] >= 0) {
+            if (i + kAhead < hi && off[i + kAhead] >= 0) {
                 int sa;
                 const uint16_t *pa = roi_src(c[i + kAhead], sa);
                 for (int j = 0; j < sa; ++j) {
@@ -191,26 +225,24 @@ RoiPlan plan_and_gather_rois(const uint16_t *frames, int n_frames, int n_rows, i
                     __builtin_prefetch(pa + (size_t)j * n_rows + sa - 1);
                 }
             }
-            if (slot_of[i] < 0) continue;
-            const int slot = (slot_of[i] += base[t]);
+            if (off[i] < 0) continue;
             int sd;
             const uint16_t *src = roi_src(c[i], sd);
-            uint16_t *dst = dst0 + (size_t)slot * side * side;
-            for (int j = 0; j < sd; ++j)
-                std::memcpy(dst + (size_t)j * side, src + (size_t)j * n_rows, (size_t)sd * sizeof(uint16_t));
+            off[i] = (int)at;
+            copy_roi(dst0 + at, src, sd, (size_t)n_rows, end);
+            at += (long long)sd * sd;
         }
     });
     plan.use = true;
-    plan.slots = total;
-    plan.side = side;
+    plan.px = total;
     return plan;
 }
 
 // the pixel view a fit call reads in ROI mode
 struct RoiView {
-    const int *slot;
+    const int *off;
     const uint16_t *stack;
-    int side, slots;
+    long long px;
 };
 
 }  // namespace
@@ -437,10 +469,9 @@ int fit_impl(loc_ctx *ctx, const uint16_t *d_frames, int n_frames, int n_rows, i
     p.cands = d_cands;
     p.n_cands = n_cands;
     if (roi) {
-        p.roi_slot = roi->slot;
+        p.roi_slot = roi->off;
         p.roi_stack = roi->stack;
-        p.roi_side = roi->side;
-        p.roi_slots = roi->slots;
+        p.roi_px = roi->px;
     }
     p.method = method;
     p.w0 = w0;
@@ -757,7 +788,7 @@ LOC_API int loc_fit_host(loc_ctx *ctx, const uint16_t *frames, int n_frames, int
                                     o.host_roi_mode > 0, (int *)ctx->pin_slot.p, &ctx->pin_roi, &e);
         if (e != cudaSuccess) return fail(LOC_E_NOMEM, std::string("ROI staging: ") + cudaGetErrorString(e));
     }
-    const size_t fbytes = plan.use ? (size_t)plan.slots * plan.side * plan.side * sizeof(uint16_t)
+    const size_t fbytes = plan.use ? (size_t)plan.px * sizeof(uint16_t)
                                    : (size_t)n_frames * n_rows * n_cols * sizeof(uint16_t);
     const size_t sbytes = plan.use ? sizeof(int) * (size_t)n_cands : 0;
     if ((e = ctx->frames.ensure(fbytes ? fbytes : 1)) != cudaSuccess ||
@@ -777,7 +808,7 @@ LOC_API int loc_fit_host(loc_ctx *ctx, const uint16_t *frames, int n_frames, int
         return cuda_fail(e, "ROI slots upload");
     ctx->h2d_bytes += fbytes + cbytes + sbytes;
     ctx->d2h_bytes += obytes + (size_t)n_cands;
-    const RoiView view{(const int *)ctx->roi_slot.p, (const uint16_t *)ctx->frames.p, plan.side, plan.slots};
+    const RoiView view{(const int *)ctx->roi_slot.p, (const uint16_t *)ctx->frames.p, plan.px};
     rc = fit_impl(ctx, (const uint16_t *)ctx->frames.p, n_frames, n_rows, n_cols, (const loc_candidate *)ctx->cands.p,
                   n_cands, method, w0, sigma, opt, (double *)ctx->out.p, (uint8_t *)ctx->flags.p, st,
                   plan.use ? &view : nullptr);
@@ -824,7 +855,7 @@ LOC_API int loc_fit_host_async(loc_ctx *ctx, const uint16_t *frames, int n_frame
                                     o.host_roi_mode > 0, (int *)sl.pin_slot.p, &sl.pin_roi, &e);
         if (e != cudaSuccess) return fail(LOC_E_NOMEM, std::string("ROI staging: ") + cudaGetErrorString(e));
     }
-    const size_t fbytes = plan.use ? (size_t)plan.slots * plan.side * plan.side * sizeof(uint16_t)
+    const size_t fbytes = plan.use ? (size_t)plan.px * sizeof(uint16_t)
                                    : (size_t)n_frames * n_rows * n_cols * sizeof(uint16_t);
     const size_t sbytes = plan.use ? sizeof(int) * (size_t)n_cands : 0;
     const size_t need = locb::scratch_bytes(method, n_cands, o.precision, o.fp64_rerun >= 0 ? 1 : 0,
@@ -857,7 +888,7 @@ LOC_API int loc_fit_host_async(loc_ctx *ctx, const uint16_t *frames, int n_frame
     if ((e = cudaStreamWaitEvent(ctx->s_fit, sl.in_done, 0)) != cudaSuccess ||
         (e = cudaStreamWaitEvent(ctx->s_fit, sl.out_done, 0)) != cudaSuccess)
         return cuda_fail(e, "stream wait");
-    const RoiView view{(const int *)sl.roi_slot.p, (const uint16_t *)sl.frames.p, plan.side, plan.slots};
+    const RoiView view{(const int *)sl.roi_slot.p, (const uint16_t *)sl.frames.p, plan.px};
     if (n_cands > 0)
         rc = fit_impl(ctx, (const uint16_t *)sl.frames.p, n_frames, n_rows, n_cols, (const loc_candidate *)sl.cands.p,
                       n_cands, method, w0, sigma, opt, (double *)sl.out.p, (uint8_t *)sl.flags.p, ctx->s_fit,

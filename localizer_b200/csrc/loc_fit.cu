@@ -49,11 +49,11 @@ struct K0Args {
     int *cls;
     int *meta;
     int *cls2;   // optional: FP64 re-run marks, cleared here
-    // ROI mode: a candidate that passes the edge rule must have a slot of a
-    // side that holds its ROI (else it is flagged as bad input: the solver
-    // never reads outside the slots)
+    // ROI mode: a candidate that passes the edge rule must have its ROI
+    // inside the packed ROI stack (else it is flagged as bad input: the
+    // solver never reads outside the stack)
     const int *roi_slot;
-    int roi_slots, roi_rmax;
+    long long roi_px;
 };
 
 __device__ void write_reject_row(double *row, int ncol_total, int frame)
@@ -84,7 +84,8 @@ __global__ void k0_classify(K0Args a)
             const double xm = xo + 2 * r, ym = yo + 2 * r;
             if (xo < 0 || xm > a.n_rows - 1 || yo < 0 || ym > a.n_cols - 1) {
                 flag = F_EDGE;
-            } else if (a.roi_slot && (a.roi_slot[i] < 0 || a.roi_slot[i] >= a.roi_slots || r > a.roi_rmax)) {
+            } else if (a.roi_slot && (a.roi_slot[i] < 0 ||
+                                      (long long)a.roi_slot[i] + (long long)(2 * r + 1) * (2 * r + 1) > a.roi_px)) {
                 flag = F_BAD_INPUT;
             } else {
                 cls = r;
@@ -268,7 +269,7 @@ struct K1Args {
     float *cont_state;  // saved solver state of suspended fits
     int cont_stride;
     int compensated;    // FP32 solver: sum the group's partial normal equations in FP64
-    const int *roi_slot;  // ROI mode: slot of each candidate (frame_px = slot pixels, n_rows = slot side)
+    const int *roi_slot;  // ROI mode: first pixel of each candidate's packed ROI (row pitch 2r + 1)
 };
 
 template <int METHOD, int S, int TPF, typename T> struct Pass;
@@ -587,11 +588,12 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
                     }
                     phase = 1;
                 }
-                rbase = a.roi_slot ? (long long)a.roi_slot[my] * a.frame_px
+                rbase = a.roi_slot ? (long long)a.roi_slot[my]
                                    : (long long)fr * a.frame_px + xo + (long long)yo * a.n_rows;
             }
             // warp-cooperative ROI staging: global uint16 -> shared float
             unsigned got = __ballot_sync(kFull, my >= 0 && leader);
+            const int pitch = a.roi_slot ? s : a.n_rows;   // a packed ROI's rows are 2r + 1 pixels apart
             while (got) {
                 const int src = __ffs(got) - 1;
                 got &= got - 1;
@@ -600,7 +602,7 @@ __device__ __forceinline__ void run_class(const K1Args &a, int r, float *smem, u
                 float *dst = smem + ((tid - lane + src) / TPF) * stride;
                 for (int k = lane; k < npx; k += 32) {
                     const int j = k / s, i = k - j * s;
-                    dst[k] = (float)__ldg(fb + i + (size_t)j * a.n_rows);
+                    dst[k] = (float)__ldg(fb + i + (size_t)j * pitch);
                 }
             }
             __syncwarp();
@@ -1316,11 +1318,10 @@ cudaError_t enqueue_fit(const FitParams &p, const Scratch &s, cudaStream_t strea
     // the start proposal cuts its windows from whole frames
     if (roi_mode && p.warm) return cudaErrorInvalidValue;
     const uint16_t *px = roi_mode ? p.roi_stack : p.frames;
-    const long long px_frame = roi_mode ? (long long)p.roi_side * p.roi_side : (long long)p.n_rows * p.n_cols;
-    const int px_pitch = roi_mode ? p.roi_side : p.n_rows;
+    const long long px_frame = roi_mode ? 0 : (long long)p.n_rows * p.n_cols;
+    const int px_pitch = roi_mode ? 0 : p.n_rows;   // ROI mode: each ROI's own side
     K0Args k0{(const Cand *)p.cands, n, p.n_frames, p.n_rows, p.n_cols, r_default, r_cap, p.method, ncol_total,
-              p.out, p.flags, s.cls, s.meta, rerun ? s.cls2 : nullptr, p.roi_slot, p.roi_slots,
-              (p.roi_side - 1) / 2};
+              p.out, p.flags, s.cls, s.meta, rerun ? s.cls2 : nullptr, p.roi_slot, p.roi_px};
     const int nb = (n + 255) / 256;
     k0_classify<<<nb, 256, 0, stream>>>(k0);
     k0_classes<<<1, 32, 0, stream>>>(s.meta);

@@ -78,14 +78,15 @@ struct FitParams {
     cudaEvent_t join_long[kMaxAux];
     double *out;
     uint8_t *flags;
-    // ROI mode (host-buffer calls): the pixels are not whole frames but one
-    // roi_side x roi_side slot per candidate, candidate i's ROI in slot
-    // roi_slot[i] with its origin at the slot's first pixel (roi_slot NULL:
-    // frame mode). Frames, n_frames, n_rows and n_cols above still describe
-    // the original stack (the edge and input rules use them).
+    // ROI mode (host-buffer calls): the pixels are not whole frames but the
+    // candidates' ROIs packed one after another, candidate i's (2r+1)^2 ROI
+    // (row pitch 2r+1, x fastest) starting at pixel roi_slot[i] of roi_stack,
+    // which holds roi_px pixels (roi_slot NULL: frame mode). Frames,
+    // n_frames, n_rows and n_cols above still describe the original stack
+    // (the edge and input rules use them).
     const int *roi_slot;
     const uint16_t *roi_stack;
-    int roi_side, roi_slots;
+    long long roi_px;
 };
 
 int state_stride(int method);

@@ -1,6 +1,6 @@
 """ROI mode of the host-buffer calls: when the candidates' ROIs are a small
-part of the frames, loc_fit_host and loc_fit_host_async copy one slot per
-candidate instead of the frames. The rows and flags must be those of the
+part of the frames, loc_fit_host and loc_fit_host_async copy the candidates'
+ROIs, packed each at its own size, instead of the frames. The rows and flags must be those of the
 whole-frame upload (host_roi_mode = -1) and of the device-pointer call, bit
 for bit, including the candidates the input and edge rules reject before any
 pixel is read, mixed ROI half-widths, and a caller's half-width cap."""
@@ -55,6 +55,10 @@ def test_roi_mode_rows_match_frame_upload(engine, name, method):
     np.testing.assert_array_equal(rows_r, rows_f)
     assert h1 - h0 >= frames.nbytes
     assert h2 - h1 < frames.nbytes + cands.nbytes + 4 * len(cands)   # ROI mode was taken
+    # the packed stack holds exactly the (2r+1)^2 pixels of each candidate that reads pixels
+    r = np.where(cands["half_width"] > 0, cands["half_width"], int(np.ceil(4 * w.w0)))
+    reads = (flags_r != 1) & (flags_r != 10)
+    assert h2 - h1 == 2 * int(((2 * r[reads] + 1) ** 2).sum()) + cands.nbytes + 4 * len(cands)
     # the rejects: edge (2), bad input (NaN, frame range, half-width above the cap)
     assert list(flags_r[-7:]) == [1, 1, 10, 1, 10, 10, 10]
 
@@ -110,7 +114,7 @@ def test_roi_mode_async_stream_of_stacks(engine):
 
 def test_dense_candidates_fall_back_to_frames(engine):
     """Candidates whose ROIs cover the frames several times over: the whole
-    frames are copied even when ROI mode is asked for (the slots would be
+    frames are copied even when ROI mode is asked for (the ROI stack would be
     larger)."""
     w, frames, _ = _stack("small", 4, 730)
     n_frames, n_cols, n_rows = frames.shape
