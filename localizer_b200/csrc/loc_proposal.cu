@@ -11,9 +11,12 @@
 //
 // Network (valid 3x3 convolutions, ReLU after each):
 //   window 1x11x11 -> conv1 16x9x9 -> conv2 32x7x7 -> conv3 32x5x5 -> linear(800 -> P)
-// conv1 (one input channel, 9 taps) and the linear head run on the CUDA cores
-// in FP32; conv2 and conv3 (K = 144 and 288) run on the 5th-generation tensor
-// cores (tcgen05.mma, BF16 operands, FP32 accumulation in tensor memory).
+// The three convolutions run on the 5th-generation tensor cores
+// (tcgen05.mma, BF16 operands, FP32 accumulation in tensor memory): conv1
+// (one input channel) as an im2col GEMM with its 9 taps padded to K = 16,
+// conv2 and conv3 (K = 144 and 288) as implicit GEMMs; the linear head runs on
+// the CUDA cores in FP32. The window pixels of a CTA's next group are loaded
+// into registers while the current group is processed.
 //
 // Implicit GEMM without im2col: activations of R windows live in shared
 // memory on a 9-wide grid, one row per grid position (81 rows per window,
@@ -66,9 +69,9 @@ constexpr int kRows = 81 * kR;                    // activation grid rows per it
 constexpr int kTiles = (kRows + 127) / 128;       // M = 128 tiles
 constexpr int kRowsAlloc = kTiles * 128 + 24;     // + largest tap shift (20), multiple of 8
 constexpr uint32_t kLBO = kRowsAlloc * 16;        // bytes between 8-channel chunks
-constexpr uint32_t kTmemCols = 256;
+constexpr uint32_t kTmemCols = kTiles * 32 <= 32 ? 32 : kTiles * 32 <= 64 ? 64 : kTiles * 32 <= 128 ? 128 : 256;
 static_assert(kTiles * 32 <= (int)kTmemCols, "accumulators must fit in tensor memory");
-constexpr int kThreads = 128;               // 4 warps: one TMEM lane quarter each
+constexpr int kThreads = 256;               // 8 warps: two per TMEM lane quarter
 constexpr int kCtasPerSm = 2;               // two CTAs per SM overlap tensor and CUDA-core phases
 constexpr int kBwdThreads = 256;            // backward pass block (its conv1 step uses 160 threads)
 constexpr float kSigmaRef = 1.5f;
@@ -84,10 +87,12 @@ constexpr int kB3 = 14016;    // [32]
 constexpr int kWH = 14048;    // [P][32][25]   head (output, channel, position)
 __host__ __device__ constexpr int weight_count(int nout) { return kWH + nout * 800 + nout; }
 
-// packed BF16 operands, K-major chunks: conv2 [tap][chunk 2][out 32][8], conv3 [tap][chunk 4][out 32][8]
+// packed BF16 operands, K-major chunks: conv2 [tap][chunk 2][out 32][8], conv3 [tap][chunk 4][out 32][8],
+// conv1 [chunk 2][out 16][8] (K = tap, taps 9..15 zero)
 constexpr int kW2P = 9 * 2 * 32 * 8;
 constexpr int kW3P = 9 * 4 * 32 * 8;
-constexpr int kWP = kW2P + kW3P;
+constexpr int kW1P = 2 * 16 * 8;
+constexpr int kWP = kW2P + kW3P + kW1P;
 
 // forward kernel shared memory (bytes)
 constexpr int SO_ACT1 = 0;
@@ -98,13 +103,17 @@ constexpr int SO_W1 = SO_V + kR * kWin2 * 4;      // w1 + b1
 constexpr int SO_B23 = SO_W1 + 160 * 4;           // b2 + b3
 constexpr int SO_HACC = SO_B23 + 64 * 4;          // head outputs (head weights are read through L1)
 constexpr int SO_STAT = SO_HACC + kR * 8 * 4;
-constexpr int SO_BAR = SO_STAT + kR * 4 * 4;
+constexpr int SO_ORG = SO_STAT + kR * 4 * 4;       // next group's window origins
+constexpr int SO_BAR = SO_ORG + kR * 4 * 4;
 constexpr int SO_MISC = SO_BAR + 8;
 constexpr int kSmemFwd = SO_MISC + 16;
-static_assert(kCtasPerSm * (kSmemFwd + 1024) <= 228 * 1024, "two forward CTAs per SM");
+static_assert(kCtasPerSm * (kSmemFwd + 1024) <= 228 * 1024, "forward CTAs per SM: shared memory");
+static_assert(kCtasPerSm * (int)kTmemCols <= 512, "forward CTAs per SM: tensor memory");
 static_assert(SO_ACT2 % 16 == 0 && SO_WP % 16 == 0 && SO_V % 16 == 0 && SO_BAR % 8 == 0, "alignment");
 
 constexpr uint32_t kIdesc = tc::idesc_bf16_f32<128, 32>();
+constexpr uint32_t kIdesc1 = tc::idesc_bf16_f32<128, 16>();
+constexpr int kPre = (kR * kWin2 + kThreads - 1) / kThreads;   // prefetched window pixels per thread
 constexpr int kA3Stride = 808;   // floats per window of conv3 output in shared memory (800 + bank padding)
 static_assert(kR * kA3Stride * 4 <= 4 * (int)kLBO, "conv3 outputs fit in the conv2 activation buffer");
 
@@ -248,19 +257,23 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
     const uint32_t tmem = *tslot;
     uint32_t phase = 0;
     bool failed = false;
-    const int q = warp;   // epilogue: the warp's TMEM lane quarter (4 warps)
+    // epilogues: a warp reads its TMEM lane quarter; with more than 4 warps,
+    // the warps of one quarter split the accumulator columns between them
+    constexpr int kEpiSets = kThreads / 128;
+    static_assert(kEpiSets * 128 == kThreads && (kEpiSets == 1 || kEpiSets == 2), "epilogue warp sets");
+    const int q = warp & 3, eset = warp >> 2;
     const uint32_t t_lane = (uint32_t)(32 * q) << 16;
     const float *bh = wh + NOUT * 800;
 
     const int ngroups = (a.n + kR - 1) / kR;
-    for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
-        const int base = g * kR;
-        // ---- 1. windows (raw counts) ----
-        int *org = reinterpret_cast<int *>(stat);  // per window: x0, y0, frame (-1: none); stat is rewritten below
+    // window origins of group g (x0, y0, frame or ROI index; -1: none) into
+    // orgn, by the first kR threads
+    int *orgn = reinterpret_cast<int *>(sm + SO_ORG);
+    auto set_origins = [&](int g) {
         if (tid < kR) {
-            const int item = base + tid;
+            const int item = g * kR + tid;
             int x0 = 0, y0 = 0, fr = -1;
-            if (item < a.n) {
+            if (g < ngroups && item < a.n) {
                 if constexpr (MODE == 0) {
                     fr = a.index ? a.index[item] : item;
                 } else if (a.cls[item] >= 0) {
@@ -270,28 +283,52 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
                     fr = c.frame;
                 }
             }
-            org[tid * 4 + 0] = x0;
-            org[tid * 4 + 1] = y0;
-            org[tid * 4 + 2] = fr;
+            orgn[tid * 4 + 0] = x0;
+            orgn[tid * 4 + 1] = y0;
+            orgn[tid * 4 + 2] = fr;
         }
-        __syncthreads();
-        for (int k = tid; k < kR * kWin2; k += kThreads) {
-            const int rr = k / kWin2, px = k - rr * kWin2, jy = px / kWin, ix = px - jy * kWin;
-            const int fr = org[rr * 4 + 2];
-            float val = 0.f;
-            if (fr >= 0) {
-                if constexpr (MODE == 0) {
-                    val = (float)__ldg(a.rois + (size_t)fr * kWin2 + px);
-                } else {
-                    const int xx = min(max(org[rr * 4 + 0] + ix, 0), a.n_rows - 1);
-                    const int yy = min(max(org[rr * 4 + 1] + jy, 0), a.n_cols - 1);
-                    val = (float)__ldg(a.frames + (size_t)fr * (size_t)a.frame_px + xx + (size_t)yy * a.n_rows);
+    };
+    // the raw window pixels of the group whose origins are in orgn, into
+    // registers (consumed one group later, so the loads' latency is hidden
+    // behind the current group's work)
+    uint16_t pre[kPre];
+    auto fetch_windows = [&]() {
+#pragma unroll
+        for (int i = 0; i < kPre; ++i) {
+            const int k = tid + i * kThreads;
+            uint16_t val = 0;
+            if (k < kR * kWin2) {
+                const int rr = k / kWin2, px = k - rr * kWin2;
+                const int fr = orgn[rr * 4 + 2];
+                if (fr >= 0) {
+                    if constexpr (MODE == 0) {
+                        val = __ldg(a.rois + (size_t)fr * kWin2 + px);
+                    } else {
+                        const int jy = px / kWin, ix = px - jy * kWin;
+                        const int xx = min(max(orgn[rr * 4 + 0] + ix, 0), a.n_rows - 1);
+                        const int yy = min(max(orgn[rr * 4 + 1] + jy, 0), a.n_cols - 1);
+                        val = __ldg(a.frames + (size_t)fr * (size_t)a.frame_px + xx + (size_t)yy * a.n_rows);
+                    }
                 }
             }
-            v[k] = val;
+            pre[i] = val;
         }
+    };
+    set_origins(blockIdx.x);
+    __syncthreads();
+    fetch_windows();
+    __syncthreads();   // every thread has read orgn before the loop rewrites it
+    for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        const int base = g * kR;
+        // ---- 1. windows (raw counts) from the prefetched registers ----
+#pragma unroll
+        for (int i = 0; i < kPre; ++i) {
+            const int k = tid + i * kThreads;
+            if (k < kR * kWin2) v[k] = (float)pre[i];
+        }
+        set_origins(g + (int)gridDim.x);
         __syncthreads();
-        // ---- 2. normalisation statistics, two windows per warp ----
+        // ---- 2. normalisation statistics, one warp per window ----
         for (int rr = warp; rr < kR; rr += kThreads / 32) {
             const float *wv = v + rr * kWin2;
             float sb = 0.f, sc = 0.f;
@@ -312,9 +349,11 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
             }
         }
         __syncthreads();
+        fetch_windows();   // the next group's pixels, in flight during this group's work
+        // normalised pixels, rounded to BF16 (conv1's tensor-core operand)
         for (int k = tid; k < kR * kWin2; k += kThreads) {
             const int rr = k / kWin2;
-            const float nv = (v[k] - stat[rr * 4]) * stat[rr * 4 + 2];
+            const float nv = __bfloat162float(__float2bfloat16_rn((v[k] - stat[rr * 4]) * stat[rr * 4 + 2]));
             v[k] = nv;
             if constexpr (MODE == 0) {
                 if (a.save_v && base + rr < a.n) a.save_v[(size_t)base * kWin2 + k] = nv;
@@ -327,33 +366,62 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
             }
         }
         __syncthreads();
-        // ---- 3. conv1 on the CUDA cores -> act1 (BF16, K-major chunks) ----
-        for (int m = tid; m < kRows; m += kThreads) {
-            const int rr = m / 81, pos = m - rr * 81, iy = pos / 9, ix = pos - iy * 9;
-            const float *wv = v + rr * kWin2 + iy * kWin + ix;
-            float x9[9];
-#pragma unroll
-            for (int t = 0; t < 9; ++t) x9[t] = wv[(t / 3) * kWin + t % 3];
-            uint32_t pk[8];
-#pragma unroll
-            for (int co = 0; co < 16; co += 2) {
-                float z0 = w1[144 + co], z1 = w1[144 + co + 1];
-#pragma unroll
-                for (int t = 0; t < 9; ++t) {
-                    z0 = fmaf(w1[co * 9 + t], x9[t], z0);
-                    z1 = fmaf(w1[(co + 1) * 9 + t], x9[t], z1);
-                }
-                pk[co / 2] = pack_bf16x2(fmaxf(z0, 0.f), fmaxf(z1, 0.f));
+        // ---- 3. conv1 on the tensor cores: im2col rows (9 taps + 7 zeros, BF16)
+        // in the conv2 activation buffer (free until the conv2 epilogue) ----
+        for (int m = tid; m < kTiles * 128; m += kThreads) {
+            uint4 c0 = make_uint4(0, 0, 0, 0), c1 = c0;
+            if (m < kRows) {
+                const int rr = m / 81, pos = m - rr * 81, iy = pos / 9, ix = pos - iy * 9;
+                const float *wv = v + rr * kWin2 + iy * kWin + ix;
+                c0 = make_uint4(pack_bf16x2(wv[0], wv[1]), pack_bf16x2(wv[2], wv[kWin]),
+                                pack_bf16x2(wv[kWin + 1], wv[kWin + 2]), pack_bf16x2(wv[2 * kWin], wv[2 * kWin + 1]));
+                c1.x = pack_bf16x2(wv[2 * kWin + 2], 0.f);
             }
-            const uint4 c0 = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-            const uint4 c1 = make_uint4(pk[4], pk[5], pk[6], pk[7]);
-            *reinterpret_cast<uint4 *>(sm + SO_ACT1 + m * 16) = c0;
-            *reinterpret_cast<uint4 *>(sm + SO_ACT1 + kLBO + m * 16) = c1;
-            if constexpr (MODE == 0) {
-                if (a.save_a1 && base + rr < a.n) {
-                    uint4 *d = reinterpret_cast<uint4 *>(a.save_a1 + ((size_t)(base + rr) * 81 + pos) * 16);
-                    d[0] = c0;
-                    d[1] = c1;
+            *reinterpret_cast<uint4 *>(sm + SO_ACT2 + m * 16) = c0;
+            *reinterpret_cast<uint4 *>(sm + SO_ACT2 + kLBO + m * 16) = c1;
+        }
+        tc::fence_async_smem();
+        tc::fence_before_sync();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after_sync();
+            const uint32_t cb = tc::smem_addr(sm + SO_ACT2), w1 = tc::smem_addr(sm + SO_WP + (kW2P + kW3P) * 2);
+            const uint64_t bd = tc::smem_desc(w1, 256, 128);
+            for (int i = 0; i < kTiles; ++i)
+                tc::mma_bf16(tmem + (uint32_t)i * 32u, tc::smem_desc(cb + (uint32_t)i * 128u * 16u, kLBO, 128), bd,
+                             kIdesc1, 0u);
+            tc::mma_commit(bar);
+        }
+        __syncwarp();
+        if (!tc::mbar_wait(bar, phase, kWaitLimit)) failed = true;
+        phase ^= 1u;
+        if (__syncthreads_or(failed)) {
+            failed = true;
+            break;
+        }
+        tc::fence_after_sync();
+        // conv1 epilogue: bias, ReLU, BF16 -> act1 (K-major chunks)
+        for (int i = eset; i < kTiles; i += kEpiSets) {
+            float acc[16];
+            tc::tmem_ld16(tmem + t_lane + (uint32_t)(i * 32), acc);
+            tc::tmem_ld_wait();
+            const int m = i * 128 + 32 * q + lane;
+            if (m < kRows) {
+                uint32_t pk[8];
+#pragma unroll
+                for (int c = 0; c < 16; c += 2)
+                    pk[c / 2] = pack_bf16x2(fmaxf(acc[c] + w1[144 + c], 0.f), fmaxf(acc[c + 1] + w1[144 + c + 1], 0.f));
+                const uint4 c0 = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                const uint4 c1 = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+                *reinterpret_cast<uint4 *>(sm + SO_ACT1 + m * 16) = c0;
+                *reinterpret_cast<uint4 *>(sm + SO_ACT1 + kLBO + m * 16) = c1;
+                if constexpr (MODE == 0) {
+                    const int rr = m / 81, pos = m - rr * 81;
+                    if (a.save_a1 && base + rr < a.n) {
+                        uint4 *d = reinterpret_cast<uint4 *>(a.save_a1 + ((size_t)(base + rr) * 81 + pos) * 16);
+                        d[0] = c0;
+                        d[1] = c1;
+                    }
                 }
             }
         }
@@ -384,7 +452,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
         tc::fence_after_sync();
         // ---- 5. conv2 epilogue: bias, ReLU, BF16 -> act2 ----
         for (int i = 0; i < kTiles; ++i)
-        for (int h = 0; h < 2; ++h) {
+        for (int h = eset; h < 2; h += kEpiSets) {
             float acc[16];
             tc::tmem_ld16(tmem + t_lane + (uint32_t)(i * 32 + 16 * h), acc);
             tc::tmem_ld_wait();
@@ -443,7 +511,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
         // activation buffers are free once the conv3 MMAs have completed) ----
         float *a3s = reinterpret_cast<float *>(sm + SO_ACT2);   // [kR][kA3Stride], (channel, position)
         for (int i = 0; i < kTiles; ++i)
-        for (int h = 0; h < 2; ++h) {
+        for (int h = eset; h < 2; h += kEpiSets) {
             float acc[16];
             tc::tmem_ld16(tmem + t_lane + (uint32_t)(i * 32 + 16 * h), acc);
             tc::tmem_ld_wait();
@@ -470,15 +538,16 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
         }
         tc::fence_before_sync();
         __syncthreads();
-        // ---- head: 16 threads per window, each over every 16th feature ----
+        // ---- head: kTPW threads per window, each over every kTPW-th feature ----
         {
-            static_assert(kThreads == 16 * kR, "head mapping");
-            const int rr = tid >> 4, sub = tid & 15;
+            constexpr int kTPW = kThreads / kR;
+            static_assert(kTPW * kR == kThreads && kTPW <= 32 && (kTPW & (kTPW - 1)) == 0, "head mapping");
+            const int rr = tid / kTPW, sub = tid % kTPW;
             const float *x = a3s + rr * kA3Stride;
             float part[NOUT];
 #pragma unroll
             for (int j = 0; j < NOUT; ++j) part[j] = 0.f;
-            for (int f = sub; f < 800; f += 16) {
+            for (int f = sub; f < 800; f += kTPW) {
                 const float xv = x[f];
 #pragma unroll
                 for (int j = 0; j < NOUT; ++j) part[j] = fmaf(wh[j * 800 + f], xv, part[j]);
@@ -486,10 +555,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
 #pragma unroll
             for (int j = 0; j < NOUT; ++j) {
                 float t = part[j];
-                t += __shfl_xor_sync(0xffffffffu, t, 8);
-                t += __shfl_xor_sync(0xffffffffu, t, 4);
-                t += __shfl_xor_sync(0xffffffffu, t, 2);
-                t += __shfl_xor_sync(0xffffffffu, t, 1);
+#pragma unroll
+                for (int o = kTPW / 2; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
                 if (sub == 0) hacc[rr * 8 + j] = t;
             }
         }
@@ -793,10 +860,14 @@ __global__ void k_pack(const float *w, __nv_bfloat16 *wp)
     if (i < kW2P) {
         const int e = i & 7, co = (i >> 3) & 31, c = (i >> 8) & 1, t = i >> 9;
         wp[i] = __float2bfloat16_rn(w[kW2 + (co * 16 + c * 8 + e) * 9 + t]);
-    } else if (i < kWP) {
+    } else if (i < kW2P + kW3P) {
         const int k = i - kW2P;
         const int e = k & 7, co = (k >> 3) & 31, c = (k >> 8) & 3, t = k >> 10;
         wp[i] = __float2bfloat16_rn(w[kW3 + (co * 32 + c * 8 + e) * 9 + t]);
+    } else if (i < kWP) {
+        const int k = i - kW2P - kW3P;
+        const int e = k & 7, co = (k >> 3) & 15, t = (k >> 7) * 8 + e;
+        wp[i] = __float2bfloat16_rn(t < 9 ? w[kW1 + co * 9 + t] : 0.f);
     }
 }
 

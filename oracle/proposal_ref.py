@@ -14,7 +14,8 @@ documents:
   linear head 800 -> P over the (channel, position) flattening.
 
 With ``bf16=True`` the values the GPU rounds to BF16 are rounded the same way
-(round to nearest even): the conv2 and conv3 weights and the conv1 and conv2
+(round to nearest even): the normalised window and the conv1 weights (conv1's
+tensor-core operands), the conv2 and conv3 weights and the conv1 and conv2
 activations. Everything else is FP64. The backward pass treats the rounding
 as the identity (as the GPU's does) and ReLU's derivative as 1 where the
 activation is positive.
@@ -101,7 +102,8 @@ def forward(w, windows, nout, bf16_round=True):
     p = unpack(w, nout)
     rnd = bf16 if bf16_round else (lambda a: np.asarray(a, dtype=np.float64))
     v, b0, s0 = normalise(windows)
-    z1 = _conv(v[:, None], p["W1"][:, None, :], p["b1"], 9)
+    v = rnd(v)
+    z1 = _conv(v[:, None], rnd(p["W1"])[:, None, :], p["b1"], 9)
     a1 = rnd(np.maximum(z1, 0.0))
     W2, W3 = rnd(p["W2"]), rnd(p["W3"])
     z2 = _conv(a1, W2, p["b2"], 7)
