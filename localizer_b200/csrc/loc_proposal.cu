@@ -94,6 +94,21 @@ constexpr int kW3P = 9 * 4 * 32 * 8;
 constexpr int kW1P = 2 * 16 * 8;
 constexpr int kWP = kW2P + kW3P + kW1P;
 
+// Raw pixels staged per window: a 15 x 15 region centred like the window,
+// which holds the 11 x 11 network window at offset (2, 2) and, for ROI
+// half-widths up to 6, the whole ROI the start check evaluates.
+constexpr int kReg = 15, kReg2 = kReg * kReg;
+constexpr int kRegOff = (kReg - kWin) / 2;
+
+// One window's record, filled one group ahead: region origin in the frame,
+// frame (or ROI index; -1: no window), the candidate's ROI half-width
+// (-1: rejected before the fit) and the fields the start check needs.
+struct WinRec {
+    double cx, cy;
+    float intensity, background;
+    int x0, y0, frame, r;
+};
+
 // forward kernel shared memory (bytes)
 constexpr int SO_ACT1 = 0;
 constexpr int SO_ACT2 = SO_ACT1 + 2 * (int)kLBO;
@@ -103,17 +118,19 @@ constexpr int SO_W1 = SO_V + kR * kWin2 * 4;      // w1 + b1
 constexpr int SO_B23 = SO_W1 + 160 * 4;           // b2 + b3
 constexpr int SO_HACC = SO_B23 + 64 * 4;          // head outputs (head weights are read through L1)
 constexpr int SO_STAT = SO_HACC + kR * 8 * 4;
-constexpr int SO_ORG = SO_STAT + kR * 4 * 4;       // next group's window origins
-constexpr int SO_BAR = SO_ORG + kR * 4 * 4;
+constexpr int SO_RAW = SO_STAT + kR * 4 * 4;       // raw pixel regions of the current group
+constexpr int SO_WIN = SO_RAW + ((kR * kReg2 * 2 + 15) / 16) * 16;   // window records: [current, next][kR]
+constexpr int SO_BAR = SO_WIN + 2 * kR * (int)sizeof(WinRec);
 constexpr int SO_MISC = SO_BAR + 8;
 constexpr int kSmemFwd = SO_MISC + 16;
 static_assert(kCtasPerSm * (kSmemFwd + 1024) <= 228 * 1024, "forward CTAs per SM: shared memory");
 static_assert(kCtasPerSm * (int)kTmemCols <= 512, "forward CTAs per SM: tensor memory");
-static_assert(SO_ACT2 % 16 == 0 && SO_WP % 16 == 0 && SO_V % 16 == 0 && SO_BAR % 8 == 0, "alignment");
+static_assert(SO_ACT2 % 16 == 0 && SO_WP % 16 == 0 && SO_V % 16 == 0 && SO_WIN % 8 == 0 && SO_BAR % 8 == 0,
+              "alignment");
 
 constexpr uint32_t kIdesc = tc::idesc_bf16_f32<128, 32>();
 constexpr uint32_t kIdesc1 = tc::idesc_bf16_f32<128, 16>();
-constexpr int kPre = (kR * kWin2 + kThreads - 1) / kThreads;   // prefetched window pixels per thread
+constexpr int kPre = (kR * kReg2 + kThreads - 1) / kThreads;   // prefetched region pixels per thread
 constexpr int kA3Stride = 808;   // floats per window of conv3 output in shared memory (800 + bank padding)
 static_assert(kR * kA3Stride * 4 <= 4 * (int)kLBO, "conv3 outputs fit in the conv2 activation buffer");
 
@@ -161,22 +178,32 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi)
     return *reinterpret_cast<const uint32_t *>(&h);
 }
 
-// Gaussian model value of a parameter vector at ROI-local pixel (i, j)
-template <int P> __device__ __forceinline__ float model_at(const float (&t)[7], float w0, float i, float j)
+// The method's Gaussian of a parameter vector (amplitude, width(s), centre,
+// correlation, offset in the method's order) as
+// A exp(qa u^2 + qb u w + qc w^2) + b with u = i - x0, w = j - y0, so that
+// evaluating it over a ROI takes no division per pixel
+struct GaussQ {
+    float A, b, qa, qb, qc, x0, y0;
+};
+template <int P> __device__ __forceinline__ GaussQ gauss_q(const float (&t)[7], float w0)
 {
     if constexpr (P == 5) {
-        const float u = i - t[2], w = j - t[3];
-        return t[0] * __expf(-(u * u + w * w) / (2.f * t[1] * t[1])) + t[4];
+        const float h = -0.5f / (t[1] * t[1]);
+        return GaussQ{t[0], t[4], h, 0.f, h, t[2], t[3]};
     } else if constexpr (P == 4) {
-        const float u = i - t[1], w = j - t[2];
-        return t[0] * __expf(-(u * u + w * w) / (2.f * w0 * w0)) + t[3];
+        const float h = -0.5f / (w0 * w0);
+        return GaussQ{t[0], t[3], h, 0.f, h, t[1], t[2]};
     } else {
-        const float u = i - t[3], w = j - t[4];
-        const float sx = t[1], sy = t[2], rho = t[5];
-        const float k = 1.f / (1.f - rho * rho);
-        const float qf = u * u / (sx * sx) - 2.f * rho * u * w / (sx * sy) + w * w / (sy * sy);
-        return t[0] * __expf(-0.5f * k * qf) + t[6];
+        // exponent -(u^2/sx^2 - 2 rho u w/(sx sy) + w^2/sy^2) / (2 (1 - rho^2))
+        const float k = 1.f / (1.f - t[5] * t[5]);
+        return GaussQ{t[0], t[6], -0.5f * k / (t[1] * t[1]), k * t[5] / (t[1] * t[2]), -0.5f * k / (t[2] * t[2]),
+                      t[3], t[4]};
     }
+}
+__device__ __forceinline__ float gauss_at(const GaussQ &g, float i, float j)
+{
+    const float u = i - g.x0, w = j - g.y0;
+    return g.A * __expf(fmaf(g.qa * u, u, fmaf(g.qb * u, w, g.qc * w * w))) + g.b;
 }
 
 struct FwdArgs {
@@ -266,47 +293,57 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
     const float *bh = wh + NOUT * 800;
 
     const int ngroups = (a.n + kR - 1) / kR;
-    // window origins of group g (x0, y0, frame or ROI index; -1: none) into
-    // orgn, by the first kR threads
-    int *orgn = reinterpret_cast<int *>(sm + SO_ORG);
+    // records of group g's windows into win_next, by the first kR threads
+    WinRec *win_cur = reinterpret_cast<WinRec *>(sm + SO_WIN);
+    WinRec *win_next = win_cur + kR;
+    uint16_t *raw = reinterpret_cast<uint16_t *>(sm + SO_RAW);
     auto set_origins = [&](int g) {
         if (tid < kR) {
             const int item = g * kR + tid;
-            int x0 = 0, y0 = 0, fr = -1;
+            WinRec w{0.0, 0.0, 0.f, 0.f, 0, 0, -1, -1};
             if (g < ngroups && item < a.n) {
                 if constexpr (MODE == 0) {
-                    fr = a.index ? a.index[item] : item;
-                } else if (a.cls[item] >= 0) {
-                    const Cand c = a.cands[item];
-                    x0 = (int)floor(c.x + 0.5) - 5;
-                    y0 = (int)floor(c.y + 0.5) - 5;
-                    fr = c.frame;
+                    w.frame = a.index ? a.index[item] : item;
+                } else {
+                    const int r = a.cls[item];
+                    if (r >= 0) {
+                        const Cand c = a.cands[item];
+                        w.cx = c.x;
+                        w.cy = c.y;
+                        w.intensity = (float)c.intensity;
+                        w.background = (float)c.background;
+                        w.x0 = (int)floor(c.x + 0.5) - 5 - kRegOff;
+                        w.y0 = (int)floor(c.y + 0.5) - 5 - kRegOff;
+                        w.frame = c.frame;
+                        w.r = r;
+                    }
                 }
             }
-            orgn[tid * 4 + 0] = x0;
-            orgn[tid * 4 + 1] = y0;
-            orgn[tid * 4 + 2] = fr;
+            win_next[tid] = w;
         }
     };
-    // the raw window pixels of the group whose origins are in orgn, into
+    // the raw region pixels of the group whose records are in win_next, into
     // registers (consumed one group later, so the loads' latency is hidden
-    // behind the current group's work)
+    // behind the current group's work); pixels outside the frame repeat its
+    // edge, and a ROI-stack window (training) fills only the inner 11 x 11
     uint16_t pre[kPre];
     auto fetch_windows = [&]() {
 #pragma unroll
         for (int i = 0; i < kPre; ++i) {
             const int k = tid + i * kThreads;
             uint16_t val = 0;
-            if (k < kR * kWin2) {
-                const int rr = k / kWin2, px = k - rr * kWin2;
-                const int fr = orgn[rr * 4 + 2];
+            if (k < kR * kReg2) {
+                const int rr = k / kReg2, px = k - rr * kReg2;
+                const int jy = px / kReg, ix = px - jy * kReg;
+                const int fr = win_next[rr].frame;
                 if (fr >= 0) {
                     if constexpr (MODE == 0) {
-                        val = __ldg(a.rois + (size_t)fr * kWin2 + px);
+                        const int wx = ix - kRegOff, wy = jy - kRegOff;
+                        if (wx >= 0 && wx < kWin && wy >= 0 && wy < kWin)
+                            val = __ldg(a.rois + (size_t)fr * kWin2 + wx + wy * kWin);
                     } else {
-                        const int jy = px / kWin, ix = px - jy * kWin;
-                        const int xx = min(max(orgn[rr * 4 + 0] + ix, 0), a.n_rows - 1);
-                        const int yy = min(max(orgn[rr * 4 + 1] + jy, 0), a.n_cols - 1);
+                        const int xx = min(max(win_next[rr].x0 + ix, 0), a.n_rows - 1);
+                        const int yy = min(max(win_next[rr].y0 + jy, 0), a.n_cols - 1);
                         val = __ldg(a.frames + (size_t)fr * (size_t)a.frame_px + xx + (size_t)yy * a.n_rows);
                     }
                 }
@@ -317,24 +354,29 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
     set_origins(blockIdx.x);
     __syncthreads();
     fetch_windows();
-    __syncthreads();   // every thread has read orgn before the loop rewrites it
+    __syncthreads();   // every thread has read win_next before the loop rewrites it
     for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
         const int base = g * kR;
-        // ---- 1. windows (raw counts) from the prefetched registers ----
+        // ---- 1. raw regions (counts) from the prefetched registers ----
 #pragma unroll
         for (int i = 0; i < kPre; ++i) {
             const int k = tid + i * kThreads;
-            if (k < kR * kWin2) v[k] = (float)pre[i];
+            if (k < kR * kReg2) raw[k] = pre[i];
         }
+        if (tid < kR) win_cur[tid] = win_next[tid];   // this group's record, before the next one replaces it
         set_origins(g + (int)gridDim.x);
         __syncthreads();
+        // the 11 x 11 window inside a region
+        auto window_px = [&](int rr, int px) -> float {
+            const int jy = px / kWin, ix = px - jy * kWin;
+            return (float)raw[rr * kReg2 + (jy + kRegOff) * kReg + ix + kRegOff];
+        };
         // ---- 2. normalisation statistics, one warp per window ----
         for (int rr = warp; rr < kR; rr += kThreads / 32) {
-            const float *wv = v + rr * kWin2;
             float sb = 0.f, sc = 0.f;
             for (int px = lane; px < kWin2; px += 32) {
                 const int jy = px / kWin, ix = px - jy * kWin;
-                const float x = wv[px];
+                const float x = window_px(rr, px);
                 if (jy == 0 || jy == kWin - 1 || ix == 0 || ix == kWin - 1) sb += x;
                 if (jy >= 4 && jy <= 6 && ix >= 4 && ix <= 6) sc += x;
             }
@@ -353,7 +395,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
         // normalised pixels, rounded to BF16 (conv1's tensor-core operand)
         for (int k = tid; k < kR * kWin2; k += kThreads) {
             const int rr = k / kWin2;
-            const float nv = __bfloat162float(__float2bfloat16_rn((v[k] - stat[rr * 4]) * stat[rr * 4 + 2]));
+            const float nv =
+                __bfloat162float(__float2bfloat16_rn((window_px(rr, k - rr * kWin2) - stat[rr * 4]) * stat[rr * 4 + 2]));
             v[k] = nv;
             if constexpr (MODE == 0) {
                 if (a.save_v && base + rr < a.n) a.save_v[(size_t)base * kWin2 + k] = nv;
@@ -575,14 +618,14 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
                 const int item = base + rr;
                 if (item >= a.n) continue;
                 float *dst = a.init + (size_t)item * P;
-                const int r = a.cls[item];
+                const WinRec &c = win_cur[rr];
+                const int r = c.r;
                 if (r < 0) {
                     if (lane == 0) dst[0] = CUDART_NAN_F;
                     continue;
                 }
-                const Cand c = a.cands[item];
-                const int xo = (int)floor(c.x - (double)r), yo = (int)floor(c.y - (double)r);
-                const int cx = (int)floor(c.x + 0.5), cy = (int)floor(c.y + 0.5);
+                const int xo = (int)floor(c.cx - (double)r), yo = (int)floor(c.cy - (double)r);
+                const int cx = (int)floor(c.cx + 0.5), cy = (int)floor(c.cy + 0.5);
                 const float b0 = stat[rr * 4 + 0], s0 = stat[rr * 4 + 1];
                 float tw[7] = {0, 0, 0, 0, 0, 0, 0}, tcold[7] = {0, 0, 0, 0, 0, 0, 0};
                 bool ok = true;
@@ -596,24 +639,29 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
                 }
                 const float side = (float)(2 * r);
                 ok = ok && tw[0] > 0.f && tw[IX] >= 0.f && tw[IX] <= side && tw[IX + 1] >= 0.f && tw[IX + 1] <= side;
-                const float xl = (float)(c.x - (double)xo), yl = (float)(c.y - (double)yo);
+                const float xl = (float)(c.cx - (double)xo), yl = (float)(c.cy - (double)yo);
                 if constexpr (P == 5) {
-                    tcold[0] = (float)c.intensity; tcold[1] = a.w0; tcold[2] = xl; tcold[3] = yl;
-                    tcold[4] = (float)c.background;
+                    tcold[0] = c.intensity; tcold[1] = a.w0; tcold[2] = xl; tcold[3] = yl; tcold[4] = c.background;
                 } else if constexpr (P == 4) {
-                    tcold[0] = (float)c.intensity; tcold[1] = xl; tcold[2] = yl; tcold[3] = (float)c.background;
+                    tcold[0] = c.intensity; tcold[1] = xl; tcold[2] = yl; tcold[3] = c.background;
                 } else {
-                    tcold[0] = (float)c.intensity; tcold[1] = a.w0; tcold[2] = a.w0; tcold[3] = xl;
-                    tcold[4] = yl; tcold[5] = 0.f; tcold[6] = (float)c.background;
+                    tcold[0] = c.intensity; tcold[1] = a.w0; tcold[2] = a.w0; tcold[3] = xl;
+                    tcold[4] = yl; tcold[5] = 0.f; tcold[6] = c.background;
                 }
+                const GaussQ gw = gauss_q<P>(tw, a.w0), gc = gauss_q<P>(tcold, a.w0);
                 const int s = 2 * r + 1;
+                // the ROI's origin inside the staged region: inside it for
+                // half-widths up to 6, else the ROI is read from the frame
+                const int ox = xo - c.x0, oy = yo - c.y0;
+                const bool staged = ox >= 0 && oy >= 0 && ox + s <= kReg && oy + s <= kReg;
+                const uint16_t *rg = raw + rr * kReg2 + ox + oy * kReg;
                 const uint16_t *fb = a.frames + (size_t)c.frame * (size_t)a.frame_px + xo + (size_t)yo * a.n_rows;
                 float cw = 0.f, cc = 0.f;
                 for (int k = lane; k < s * s; k += 32) {
                     const int j = k / s, i = k - j * s;
-                    const float d = (float)__ldg(fb + i + (size_t)j * a.n_rows);
-                    const float ew = model_at<P>(tw, a.w0, (float)i, (float)j) - d;
-                    const float ec = model_at<P>(tcold, a.w0, (float)i, (float)j) - d;
+                    const float d = staged ? (float)rg[i + j * kReg] : (float)__ldg(fb + i + (size_t)j * a.n_rows);
+                    const float ew = gauss_at(gw, (float)i, (float)j) - d;
+                    const float ec = gauss_at(gc, (float)i, (float)j) - d;
                     cw = fmaf(ew, ew, cw);
                     cc = fmaf(ec, ec, cc);
                 }
