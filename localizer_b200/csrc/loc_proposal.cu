@@ -293,31 +293,42 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
     const float *bh = wh + NOUT * 800;
 
     const int ngroups = (a.n + kR - 1) / kR;
-    // records of group g's windows into win_next, by the first kR threads
+    // window records, kept by the first kR threads: the candidate data of
+    // group g is loaded into registers (load_records) one group before
+    // store_records writes it to win_next, so the loads' latency is hidden
     WinRec *win_cur = reinterpret_cast<WinRec *>(sm + SO_WIN);
     WinRec *win_next = win_cur + kR;
     uint16_t *raw = reinterpret_cast<uint16_t *>(sm + SO_RAW);
-    auto set_origins = [&](int g) {
+    int rec_src = -1;   // MODE 0: ROI index; MODE 1: the candidate's ROI half-width (-1: none)
+    Cand rec_c{};
+    auto load_records = [&](int g) {
+        rec_src = -1;
         if (tid < kR) {
             const int item = g * kR + tid;
-            WinRec w{0.0, 0.0, 0.f, 0.f, 0, 0, -1, -1};
             if (g < ngroups && item < a.n) {
                 if constexpr (MODE == 0) {
-                    w.frame = a.index ? a.index[item] : item;
+                    rec_src = a.index ? a.index[item] : item;
                 } else {
-                    const int r = a.cls[item];
-                    if (r >= 0) {
-                        const Cand c = a.cands[item];
-                        w.cx = c.x;
-                        w.cy = c.y;
-                        w.intensity = (float)c.intensity;
-                        w.background = (float)c.background;
-                        w.x0 = (int)floor(c.x + 0.5) - 5 - kRegOff;
-                        w.y0 = (int)floor(c.y + 0.5) - 5 - kRegOff;
-                        w.frame = c.frame;
-                        w.r = r;
-                    }
+                    rec_src = a.cls[item];
+                    rec_c = a.cands[item];
                 }
+            }
+        }
+    };
+    auto store_records = [&]() {
+        if (tid < kR) {
+            WinRec w{0.0, 0.0, 0.f, 0.f, 0, 0, -1, -1};
+            if constexpr (MODE == 0) {
+                w.frame = rec_src;
+            } else if (rec_src >= 0) {
+                w.cx = rec_c.x;
+                w.cy = rec_c.y;
+                w.intensity = (float)rec_c.intensity;
+                w.background = (float)rec_c.background;
+                w.x0 = (int)floor(rec_c.x + 0.5) - 5 - kRegOff;
+                w.y0 = (int)floor(rec_c.y + 0.5) - 5 - kRegOff;
+                w.frame = rec_c.frame;
+                w.r = rec_src;
             }
             win_next[tid] = w;
         }
@@ -351,7 +362,9 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
             pre[i] = val;
         }
     };
-    set_origins(blockIdx.x);
+    load_records(blockIdx.x);
+    store_records();
+    load_records(blockIdx.x + (int)gridDim.x);
     __syncthreads();
     fetch_windows();
     __syncthreads();   // every thread has read win_next before the loop rewrites it
@@ -364,7 +377,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_prop_fwd(FwdArgs a)
             if (k < kR * kReg2) raw[k] = pre[i];
         }
         if (tid < kR) win_cur[tid] = win_next[tid];   // this group's record, before the next one replaces it
-        set_origins(g + (int)gridDim.x);
+        store_records();                            // group g + grid, loaded one group ago
+        load_records(g + 2 * (int)gridDim.x);
         __syncthreads();
         // the 11 x 11 window inside a region
         auto window_px = [&](int rr, int px) -> float {
