@@ -2,7 +2,7 @@
 """Throughput of the B200 Gaussian-PSF fit engine (fits/s at the accuracy
 gate) on the synthetic workloads of the per-emitter localization path.
 
-    python bench.py [--config {1,2,3,5}] [--gpus N] [--steps K] [--warmup W]
+    python bench.py [--config {1,2,3,4,5}] [--gpus N] [--steps K] [--warmup W]
                     [--impl reference]
 
 Configurations (seeded synthetic frames, no dataset):
@@ -21,6 +21,9 @@ Configurations (seeded synthetic frames, no dataset):
     background 150, 10 % of emitters 1.5-3 px from a neighbour, sigma 1.5,
     11 x 11 ROI, method 0; the line adds the FP32 / GPU-FP64 / CPU-FP64
     precision report.
+  4: learned proposal -- configuration 2's workload, with the start-proposal
+    network trained on 2,000,000 synthetic 11 x 11 windows of the forward
+    model instead of windows cut from frames.
 
 Frames are rendered on the GPU from seeded emitters; candidates come from
 the GPU GLRT + adjacent-8 finder. A step fits every candidate of the stack
@@ -33,7 +36,9 @@ start in FP64). `value` is the plain arm; both arms' fits/s, their ratio and
 their accuracy against the reference's own fitter on a sample of the frames
 are in the line. `e2e` runs the plain fit through the host-buffer C-ABI
 calls (a stream of loc_fit_host_async calls from pinned host memory, one per
-block of frames, uploads overlapping the previous block's fit). The CPU
+method block of frames on that method's context, uploads overlapping the
+previous block's fit; where the candidates' ROIs are a small part of the
+frames the calls upload only the ROIs, gathered by host threads). The CPU
 reference arm (`--impl reference`) runs the reference's own fitter
 (Localization.cpp compiled from the reference sources into oracle/_ref) on
 all host cores, on frames of the same configuration rendered on the host,
